@@ -1,0 +1,285 @@
+"""Python binding of libhsi_b200.so (the C ABI in include/hsi_b200.h).
+
+A thin ctypes layer: torch tensors supply device memory and streams, every
+computation runs in the library's sm_100a kernels.  There is no CPU fallback:
+importing this module on a machine without the built library raises.
+
+The functions mirror the reference's launch API for the detection path
+(include/hsi/sam_cuda.hpp, detect_cuda.hpp, stats_cuda.hpp, detector.hpp in
+GokulEdakkePuram/hsi-detectors-cuda): the same operations, argument meanings
+and error behaviour (a non-zero status raises HsiError carrying the code).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libhsi_b200.so")
+
+OK = 0
+E_INVALID = 1
+E_NOT_POSITIVE_DEFINITE = 10001
+E_TIMEOUT = 10002
+E_WORKSPACE = 10003
+E_CAPACITY = 10004
+
+F32 = 0
+F16 = 1
+LOWER_IS_BETTER = 0
+HIGHER_IS_BETTER = 1
+MAX_BANDS = 256
+MAX_INLINE_FRAMES = 4
+MAX_FILTERS_PER_PASS = 16
+
+
+class HsiError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        text = _lib.hsi_status_string(status).decode() if _lib is not None else str(status)
+        super().__init__(f"{what}: status {status} ({text})" if what else f"status {status} ({text})")
+
+
+class Scene(C.Structure):
+    """hsi_scene: the synthetic scene model (csrc/synth.h)."""
+
+    _fields_ = [
+        ("bands", C.c_int32), ("n_end", C.c_int32), ("n_targets", C.c_int32),
+        ("target_frac", C.c_float), ("anomaly_frac", C.c_float), ("noise_sigma", C.c_float),
+        ("library_seed", C.c_uint64), ("frame_seed", C.c_uint64),
+    ]
+
+
+class Frame(C.Structure):
+    """hsi_frame: one frame's cube, filter bank and output maps (device pointers)."""
+
+    _fields_ = [
+        ("cube", C.c_void_p), ("plane_stride", C.c_int64),
+        ("height", C.c_int32), ("width", C.c_int32), ("bands", C.c_int32), ("dtype", C.c_int32),
+        ("sam_targets", C.c_void_p), ("sam_norms", C.c_void_p), ("num_sam", C.c_int32),
+        ("num_cem", C.c_int32), ("cem_weights", C.c_void_p),
+        ("sam_maps", C.c_void_p), ("sam_best", C.c_void_p), ("sam_best_target", C.c_void_p),
+        ("cem_maps", C.c_void_p), ("cem_best", C.c_void_p), ("cem_best_target", C.c_void_p),
+        ("map_stride", C.c_int64),
+    ]
+
+
+DETECTION_BYTES = 16
+
+_lib = None
+
+
+def build(force: bool = False) -> None:
+    """Compile the library for sm_100a with nvcc (cross-compiles without a GPU)."""
+    subprocess.run(["make", "-s", "-j8", "-C", PKG] + (["-B"] if force else []), check=True)
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {PKG}` "
+                               "(there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, i64 = C.c_void_p, C.c_int, C.c_int64
+        L.hsi_status_string.argtypes = [i32]
+        L.hsi_status_string.restype = C.c_char_p
+        L.hsi_version.restype = i32
+        L.hsi_plane_stride.argtypes = [i32, i32]
+        L.hsi_plane_stride.restype = i64
+        L.hsi_scene_spectra.argtypes = [C.POINTER(Scene), vp]
+        L.hsi_scene_spectra.restype = i32
+        L.hsi_generate.argtypes = [C.POINTER(Scene), vp, i32, i32, i64, vp, i32, i64, vp, vp]
+        L.hsi_generate.restype = i32
+        L.hsi_score_frames.argtypes = [C.POINTER(Frame), i32, vp]
+        L.hsi_score_frames.restype = i32
+        L.hsi_score_frames_device.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp]
+        L.hsi_score_frames_device.restype = i32
+        L.hsi_detect_workspace_bytes.argtypes = [i32, i32]
+        L.hsi_detect_workspace_bytes.restype = C.c_size_t
+        L.hsi_detect.argtypes = [vp, vp, i32, i32, C.c_float, i32, i32, i32, vp, vp, vp, C.c_size_t, vp]
+        L.hsi_detect.restype = i32
+        _optional_symbols(L)
+        _lib = L
+    return _lib
+
+
+def _optional_symbols(L):
+    """Entry points added after the first slice; bound when present."""
+    vp, i32, i64, f64 = C.c_void_p, C.c_int, C.c_int64, C.c_double
+    table = {
+        "hsi_stats_workspace_bytes": ([i32, i32, i32], C.c_size_t),
+        "hsi_scene_moments": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
+        "hsi_build_statistics": ([vp, vp, f64, i32, vp, vp, i32, f64, vp, vp, vp, vp, vp, vp, vp], i32),
+        "hsi_rx_ace": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, vp, i32, vp, vp, vp, vp, i64, vp], i32),
+        "hsi_rx_ace_simt": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, vp, i32, vp, vp, vp, vp, i64, vp], i32),
+        "hsi_demosaic": ([vp, i32, i32, i32, i32, vp, vp, i64, vp], i32),
+    }
+    for name, (argtypes, restype) in table.items():
+        if hasattr(L, name):
+            fn = getattr(L, name)
+            fn.argtypes = argtypes
+            fn.restype = restype
+
+
+def check(status: int, what: str = "") -> None:
+    if status != OK:
+        raise HsiError(status, what)
+
+
+def status_string(status: int) -> str:
+    return lib().hsi_status_string(status).decode()
+
+
+def version() -> int:
+    return lib().hsi_version()
+
+
+def plane_stride(height: int, width: int) -> int:
+    """Device plane stride (pixels rounded up to 32); the reference's bsq_plane_stride."""
+    return lib().hsi_plane_stride(height, width)
+
+
+# ---------------------------------------------------------------------------
+# helpers over torch tensors
+# ---------------------------------------------------------------------------
+
+def _torch():
+    import torch
+    return torch
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def scene(bands, n_targets=1, target_frac=0.005, anomaly_frac=0.0, library_seed=0x5EED0000,
+          frame_seed=0x5EED0000, n_end=6, noise_sigma=0.005) -> Scene:
+    return Scene(bands, n_end, n_targets, target_frac, anomaly_frac, noise_sigma, library_seed, frame_seed)
+
+
+def scene_spectra(sc: Scene):
+    """Host numpy array (n_end + n_targets + 1, bands): endmembers, targets, anomaly."""
+    import numpy as np
+    out = np.zeros((sc.n_end + sc.n_targets + 1, sc.bands), np.float32)
+    check(lib().hsi_scene_spectra(C.byref(sc), out.ctypes.data), "hsi_scene_spectra")
+    return out
+
+
+def scene_targets(sc: Scene):
+    """The implanted library (n_targets, bands) as a host numpy array."""
+    return scene_spectra(sc)[sc.n_end:sc.n_end + sc.n_targets].copy()
+
+
+def generate(sc: Scene, height, width, dtype=F32, pixel0=0, stride=None, out=None, truth=True,
+             device="cuda", stream=None):
+    """Generate a frame on the device.  Returns (cube (bands, stride) tensor, truth (pixels,) uint8)."""
+    torch = _torch()
+    stride = plane_stride(height, width) if stride is None else stride
+    tdt = torch.float32 if dtype == F32 else torch.float16
+    if out is None:
+        out = torch.zeros((sc.bands, stride), dtype=tdt, device=device)
+    spectra = torch.from_numpy(scene_spectra(sc)).to(device)
+    tr = torch.empty(height * width, dtype=torch.uint8, device=device) if truth else None
+    check(lib().hsi_generate(C.byref(sc), _ptr(spectra), height, width, pixel0, _ptr(out), dtype, stride,
+                             _ptr(tr), _stream(stream)), "hsi_generate")
+    return out, tr
+
+
+def target_norms(targets):
+    """L2 norm of each target, accumulated in double then narrowed (SpectralLibrary::norms)."""
+    import numpy as np
+    t = np.asarray(targets, np.float64)
+    return np.sqrt((t * t).sum(axis=1)).astype(np.float32)
+
+
+def make_frame(cube, height, width, bands, dtype=F32, stride=None, sam_targets=None, sam_norms=None,
+               cem_weights=None, sam_maps=None, sam_best=None, sam_best_target=None, cem_maps=None,
+               cem_best=None, cem_best_target=None, map_stride=None) -> Frame:
+    stride = cube.shape[-1] if stride is None else stride
+    P = height * width
+    f = Frame()
+    f.cube = cube.data_ptr()
+    f.plane_stride = stride
+    f.height, f.width, f.bands, f.dtype = height, width, bands, dtype
+    f.sam_targets = sam_targets.data_ptr() if sam_targets is not None else None
+    f.sam_norms = sam_norms.data_ptr() if sam_norms is not None else None
+    f.num_sam = 0 if sam_targets is None else sam_targets.shape[0]
+    f.cem_weights = cem_weights.data_ptr() if cem_weights is not None else None
+    f.num_cem = 0 if cem_weights is None else cem_weights.shape[0]
+    for name, t in (("sam_maps", sam_maps), ("sam_best", sam_best), ("sam_best_target", sam_best_target),
+                    ("cem_maps", cem_maps), ("cem_best", cem_best), ("cem_best_target", cem_best_target)):
+        setattr(f, name, t.data_ptr() if t is not None else None)
+    if map_stride is None:
+        maps = sam_maps if sam_maps is not None else cem_maps
+        map_stride = maps.shape[-1] if maps is not None else P
+    f.map_stride = map_stride
+    return f
+
+
+def score_frames(frames, stream=None) -> None:
+    """Score up to 4 frames whose descriptors live on the host (one launch per pass)."""
+    n = len(frames)
+    arr = (Frame * n)(*frames)
+    check(lib().hsi_score_frames(arr, n, _stream(stream)), "hsi_score_frames")
+
+
+def frame_table(frames, device="cuda"):
+    """Upload descriptors to a device table for hsi_score_frames_device."""
+    torch = _torch()
+    n = len(frames)
+    arr = (Frame * n)(*frames)
+    raw = bytes(arr)
+    host = torch.frombuffer(bytearray(raw), dtype=torch.uint8)
+    return host.to(device)
+
+
+def score_frames_device(table, num_frames, max_bands, max_sam, max_cem, dtype=F32, status=None,
+                        stream=None) -> None:
+    """Batched scoring from a device descriptor table (see frame_table).  `status`
+    (device int32 tensor, optional) receives HSI_E_INVALID for frames outside the bounds."""
+    check(lib().hsi_score_frames_device(_ptr(table), num_frames, dtype, max_bands, max_sam, max_cem,
+                                        _ptr(status), _stream(stream)), "hsi_score_frames_device")
+
+
+def detect_workspace_bytes(height, width) -> int:
+    return lib().hsi_detect_workspace_bytes(height, width)
+
+
+def detect(score, target, height, width, threshold, nms_radius=2, polarity=LOWER_IS_BETTER, capacity=4096,
+           out=None, count=None, workspace=None, stream=None):
+    """Threshold + NMS + raster-order compaction on the device.
+
+    Returns (count tensor (1,) uint32-as-int32, detections (capacity, 4) int32 view).  The count is
+    the number found (it may exceed capacity)."""
+    torch = _torch()
+    dev = score.device
+    if out is None:
+        out = torch.zeros((max(capacity, 1), 4), dtype=torch.int32, device=dev)
+    if count is None:
+        count = torch.zeros(1, dtype=torch.int32, device=dev)
+    if workspace is None:
+        workspace = torch.empty(detect_workspace_bytes(height, width), dtype=torch.uint8, device=dev)
+    check(lib().hsi_detect(_ptr(score), _ptr(target), height, width, float(threshold), nms_radius, polarity,
+                           capacity, _ptr(out), _ptr(count), _ptr(workspace), workspace.numel(),
+                           _stream(stream)), "hsi_detect")
+    return count, out
+
+
+def detections_to_numpy(count, out, capacity):
+    """Device detection list -> numpy structured array (x, y, target, score), clamped to capacity."""
+    import numpy as np
+    n = int(count.item()) & 0xFFFFFFFF
+    k = min(n, capacity)
+    raw = out[:k].cpu().numpy()
+    dt = np.dtype([("x", "<i4"), ("y", "<i4"), ("target", "<i4"), ("score", "<f4")])
+    return n, raw.view(dt).reshape(-1) if k > 0 else np.zeros(0, dt)

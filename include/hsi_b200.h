@@ -1,0 +1,201 @@
+/*
+ * hsi_b200.h - C ABI of the B200 (sm_100a) hyperspectral detection library.
+ *
+ * Everything the reference exposes for its per-frame detection path
+ * (include/hsi/sam_cuda.hpp, detect_cuda.hpp, stats_cuda.hpp, detector.hpp,
+ * detectors.hpp in GokulEdakkePuram/hsi-detectors-cuda) is reachable through
+ * these plain-C entry points: plain pointers and sizes, no C++ or CUDA types
+ * in the signatures (a stream is the CUDA runtime's opaque stream handle).
+ * The C++ drop-in layer in include/hsi/ is implemented on top of them.
+ *
+ * Conventions
+ *  - Cubes are band-sequential (BSQ): element (band b, pixel p) lives at
+ *    cube[b * plane_stride + p], p = y * width + x.
+ *  - Every device buffer is owned by the caller.  Entry points that need
+ *    scratch say so and take it as an explicit workspace argument.
+ *  - Every entry point returns an int status: 0 on success, a CUDA runtime
+ *    error code (1..9999) when the runtime reported one, or an HSI_E_* code.
+ *    Invalid arguments return 1 (cudaErrorInvalidValue), as the reference's
+ *    launchers do (src/sam.cu:376,384,392; src/detect.cu:95-97).
+ *  - All launches are asynchronous on the given stream unless stated.
+ */
+#ifndef HSI_B200_H
+#define HSI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define HSI_API __declspec(dllexport)
+#else
+#define HSI_API __attribute__((visibility("default")))
+#endif
+
+/* ABI-compatible with cudaStream_t. */
+typedef struct CUstream_st* hsi_stream_t;
+
+/* ---- status codes -------------------------------------------------------- */
+#define HSI_OK 0
+#define HSI_E_INVALID 1             /* == cudaErrorInvalidValue */
+#define HSI_E_NOT_POSITIVE_DEFINITE 10001
+#define HSI_E_TIMEOUT 10002         /* a bounded device-side wait gave up */
+#define HSI_E_WORKSPACE 10003       /* workspace missing or too small */
+#define HSI_E_CAPACITY 10004        /* a size exceeds a documented maximum */
+#define HSI_E_NO_DEVICE 10005
+
+/* ---- element types of a cube --------------------------------------------- */
+#define HSI_F32 0
+#define HSI_F16 1
+
+/* Score polarity (reference: include/hsi/types.hpp:108-117). */
+#define HSI_LOWER_IS_BETTER 0
+#define HSI_HIGHER_IS_BETTER 1
+
+/* Limits of the scoring kernels. */
+#define HSI_MAX_BANDS 256
+#define HSI_MAX_FILTERS_PER_PASS 16 /* per kind (SAM, CEM) and pass over the cube */
+
+/* One detection, 16 bytes, same layout as hsi::Detection
+ * (reference include/hsi/types.hpp:101-106). */
+typedef struct hsi_detection {
+  int32_t x;
+  int32_t y;
+  int32_t target;
+  float score;
+} hsi_detection;
+
+/* Human-readable text for a status code. */
+HSI_API const char* hsi_status_string(int status);
+
+/* Library version as 10000*major + 100*minor + patch. */
+HSI_API int hsi_version(void);
+
+/*
+ * Plane stride, in elements, of a device BSQ cube: pixels rounded up to a
+ * multiple of 32, so every band plane starts on a 128-byte boundary and can
+ * be staged by the TMA engine.  Replaces hsi::bsq_plane_stride
+ * (reference include/hsi/sam_cuda.hpp:47, src/sam.cu:338-343, which rounds
+ * to 8).
+ */
+HSI_API int64_t hsi_plane_stride(int height, int width);
+
+/* ---- synthetic scenes ------------------------------------------------------
+ * The scene model of csrc/synth.h (Dirichlet-mixed endmembers, implanted
+ * targets, anomalies, Gaussian noise).  Stands in for the reference's
+ * synthetic FrameSource (src/frame_source.cpp:149-293) with the distribution
+ * the benchmark configurations specify.
+ */
+typedef struct hsi_scene {
+  int32_t bands;
+  int32_t n_end;          /* background endmembers, 1..8 */
+  int32_t n_targets;      /* implanted library size, 0..64 */
+  float target_frac;      /* per-target implant probability per pixel */
+  float anomaly_frac;     /* anomaly probability per pixel */
+  float noise_sigma;
+  uint64_t library_seed;  /* spectra */
+  uint64_t frame_seed;    /* per-pixel draws */
+} hsi_scene;
+
+/* Host: the scene's spectra, each `bands` floats: n_end endmembers, then
+ * n_targets targets, then one anomaly spectrum ((n_end + n_targets + 1) * bands
+ * floats in total). */
+HSI_API int hsi_scene_spectra(const hsi_scene* scene, float* out);
+
+/* Device: generate pixels [pixel0, pixel0 + height*width) of a frame into a
+ * BSQ cube of element type `dtype` with plane stride `plane_stride`.
+ * `d_spectra` is the output of hsi_scene_spectra copied to the device.
+ * `d_truth` (nullable) receives one label byte per pixel: 0 background,
+ * 1 + t for target t, 255 for an anomaly. */
+HSI_API int hsi_generate(const hsi_scene* scene, const float* d_spectra, int height, int width,
+                         int64_t pixel0, void* d_cube, int dtype, int64_t plane_stride,
+                         uint8_t* d_truth, hsi_stream_t stream);
+
+/* ---- filter-bank scoring (SAM and CEM) --------------------------------------
+ * One streaming pass over a BSQ cube scores every pixel against a bank of
+ * up to 16 SAM targets and 16 CEM filters at once.  Replaces
+ * hsi::launch_sam_best (reference include/hsi/sam_cuda.hpp:91-96,
+ * src/sam.cu:371-461) and adds CEM scoring on the device (the reference has
+ * CEM only on the CPU: src/detectors_cpu.cpp:158-187).
+ *
+ * SAM: angle_t = acos(clamp(x.r_t / (|x| |r_t|), -1, 1)); a pixel or target
+ *      with zero norm scores pi/2; best = smallest angle, lowest t on ties.
+ * CEM: response_t = w_t . x on the uncentred pixel; best = largest response,
+ *      lowest t on ties.
+ *
+ * Frames with more targets than one pass holds are scored in several passes
+ * (the best-so-far is carried in the outputs), exactly like the reference's
+ * multi-pass launcher.
+ */
+typedef struct hsi_frame {
+  const void* cube;         /* device BSQ cube */
+  int64_t plane_stride;     /* elements, multiple of 8, >= height*width */
+  int32_t height;
+  int32_t width;
+  int32_t bands;            /* 1..HSI_MAX_BANDS */
+  int32_t dtype;            /* HSI_F32 or HSI_F16 */
+  /* SAM library: target-major num_sam x bands, plus each target's L2 norm */
+  const float* sam_targets;
+  const float* sam_norms;
+  int32_t num_sam;
+  /* CEM filters: target-major num_cem x bands */
+  int32_t num_cem;
+  const float* cem_weights;
+  /* outputs, each nullable */
+  float* sam_maps;          /* num_sam maps, map t at sam_maps + t*map_stride */
+  float* sam_best;          /* smallest angle per pixel */
+  int32_t* sam_best_target;
+  float* cem_maps;
+  float* cem_best;
+  int32_t* cem_best_target;
+  int64_t map_stride;       /* elements between consecutive maps (>= pixels) */
+} hsi_frame;
+
+/* Score `num_frames` frames whose descriptors are in HOST memory.  Up to
+ * HSI_MAX_INLINE_FRAMES frames travel inside the launch; more need
+ * hsi_score_frames_device. */
+#define HSI_MAX_INLINE_FRAMES 4
+HSI_API int hsi_score_frames(const hsi_frame* frames, int num_frames, hsi_stream_t stream);
+
+/* Same for a descriptor table already in DEVICE memory: up to 256 frames of
+ * uneven sizes, band counts and libraries in one persistent launch per pass.
+ * Every frame must have element type `dtype`, at most `max_bands` bands,
+ * `max_sam` SAM targets and `max_cem` CEM filters (they pick the kernel
+ * instance); a frame outside those bounds is skipped and HSI_E_INVALID is
+ * recorded in `*d_status` (a device int, nullable, left untouched on
+ * success). */
+#define HSI_MAX_TABLE_FRAMES 256
+HSI_API int hsi_score_frames_device(const hsi_frame* d_frames, int num_frames, int dtype, int max_bands,
+                                    int max_sam, int max_cem, int* d_status, hsi_stream_t stream);
+
+/* ---- detection compaction ---------------------------------------------------
+ * Threshold + non-maximum suppression + compaction of one score map into a
+ * detection list, in raster order.  Same semantics as the reference's CPU
+ * detect_cpu (src/sam_cpu.cpp:86-138): a pixel is a candidate when
+ * score <= threshold (lower is better) or score >= threshold (higher is
+ * better); with nms_radius > 0 it is dropped when an in-bounds neighbour in
+ * the (2r+1)^2 window is strictly better, or equal with a lower linear index.
+ * Replaces hsi::launch_detect (reference include/hsi/detect_cuda.hpp:16-19,
+ * src/detect.cu:43-106), whose output order is nondeterministic and which
+ * ignores polarity on the GPU.
+ *
+ * `d_count` is read as the starting offset and receives that plus the number
+ * of detections found (callers zero it first, as with the reference).  At
+ * most `capacity` entries are written; detections past capacity are counted
+ * but not written, and the ones kept are the first in raster order.
+ * `d_target` may be null (target 0 is reported).
+ */
+HSI_API size_t hsi_detect_workspace_bytes(int height, int width);
+HSI_API int hsi_detect(const float* d_score, const int32_t* d_target, int height, int width,
+                       float threshold, int nms_radius, int polarity, int capacity,
+                       hsi_detection* d_out, uint32_t* d_count, void* d_workspace,
+                       size_t workspace_bytes, hsi_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HSI_B200_H */

@@ -1,0 +1,96 @@
+"""GPU parity: detection compaction must be bit-exact against the reference's
+detect_cpu semantics (the fixtures) and the FP64 oracle's restatement of it."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu_detect(hsi, score, target, H, W, thr, r, higher, capacity=1 << 16, count0=0):
+    s = torch.from_numpy(np.ascontiguousarray(score, np.float32).reshape(-1)).cuda()
+    t = None if target is None else torch.from_numpy(np.ascontiguousarray(target, np.int32).reshape(-1)).cuda()
+    count = torch.full((1,), count0, dtype=torch.int32, device="cuda")
+    cnt, out = hsi.detect(s, t, H, W, thr, r, 1 if higher else 0, capacity, count=count)
+    torch.cuda.synchronize()
+    return hsi.detections_to_numpy(cnt, out, capacity + count0 if capacity else 0)
+
+
+def _tuples(d):
+    return [(int(r["x"]), int(r["y"]), int(r["target"]), float(r["score"])) for r in d]
+
+
+def test_golden_maps(hsi, golden):
+    score, which = golden["sam_best_score"], golden["sam_best_target"]
+    for r in (0, 1, 2, 3):
+        n, d = _gpu_detect(hsi, score, which, 24, 32, float(golden["sam_threshold"]), r, False)
+        assert _tuples(d) == _tuples(golden[f"sam_detect_r{r}"])
+    for r in (0, 2):
+        n, d = _gpu_detect(hsi, score, which, 24, 32, float(golden["sam_threshold_hi"]), r, True)
+        assert _tuples(d) == _tuples(golden[f"sam_detect_hi_r{r}"])
+
+
+def test_golden_hand_built_cases(hsi, golden):
+    z = None
+    for r in (0, 2):
+        n, d = _gpu_detect(hsi, golden["case_blob_score"], z, 9, 9, 0.1, r, False)
+        assert _tuples(d) == _tuples(golden[f"case_blob_detect_r{r}"])
+    n, d = _gpu_detect(hsi, golden["case_plateau_score"], z, 5, 5, 0.1, 2, False)
+    assert _tuples(d) == _tuples(golden["case_plateau_detect"])
+    n, d = _gpu_detect(hsi, golden["case_polarity_score"], z, 7, 7, 0.1, 1, False)
+    assert _tuples(d) == _tuples(golden["case_polarity_low"])
+    n, d = _gpu_detect(hsi, golden["case_polarity_score"], z, 7, 7, 0.9, 1, True)
+    assert _tuples(d) == _tuples(golden["case_polarity_high"])
+    n, d = _gpu_detect(hsi, golden["case_extremum_score"], z, 9, 9, 0.55, 3, True)
+    assert _tuples(d) == _tuples(golden["case_extremum_high"])
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (1, 700), (700, 1), (37, 53), (256, 256), (1024, 2048)])
+@pytest.mark.parametrize("radius", [0, 1, 2, 4])
+@pytest.mark.parametrize("higher", [False, True])
+def test_random_plateaus_bit_exact(hsi, orc, shape, radius, higher):
+    H, W = shape
+    rng = np.random.default_rng(H * 7 + W + radius)
+    # quantised values make many exact ties, exercising the index tie-break
+    score = (rng.integers(0, 40, H * W) / 40.0).astype(np.float32)
+    target = rng.integers(0, 8, H * W).astype(np.int32)
+    thr = 0.9 if higher else 0.1
+    n0, want = orc.detect(score, target, H, W, thr, radius, higher)
+    n, got = _gpu_detect(hsi, score, target, H, W, thr, radius, higher)
+    assert n == n0
+    assert _tuples(got) == _tuples(want)
+
+
+def test_capacity_overflow_keeps_raster_prefix(hsi, orc):
+    H, W = 300, 301
+    rng = np.random.default_rng(5)
+    score = rng.uniform(0, 1, H * W).astype(np.float32)
+    n0, want = orc.detect(score, None, H, W, 0.2, 0, False)
+    cap = 1000
+    assert n0 > cap
+    n, got = _gpu_detect(hsi, score, None, H, W, 0.2, 0, False, capacity=cap)
+    assert n == n0
+    assert _tuples(got[:cap]) == _tuples(want[:cap])
+
+
+def test_count_offset_and_nan(hsi, orc):
+    score = np.array([0.05, np.nan, 0.01, 0.5, np.nan, 0.02], np.float32)
+    n0, want = orc.detect(score, None, 1, 6, 0.1, 0, False)
+    s = torch.from_numpy(score).cuda()
+    count = torch.full((1,), 5, dtype=torch.int32, device="cuda")
+    out = torch.full((16, 4), -1, dtype=torch.int32, device="cuda")
+    cnt, out = hsi.detect(s, None, 1, 6, 0.1, 0, 0, 16, out=out, count=count)
+    torch.cuda.synchronize()
+    assert int(cnt.item()) == 5 + n0 == 8
+    o = out.cpu().numpy()
+    assert (o[:5] == -1).all()
+    dt = np.dtype([("x", "<i4"), ("y", "<i4"), ("target", "<i4"), ("score", "<f4")])
+    assert _tuples(o[5:8].copy().view(dt).reshape(-1)) == _tuples(want)
+
+
+def test_workspace_is_checked(hsi):
+    s = torch.zeros(64, device="cuda")
+    small = torch.empty(8, dtype=torch.uint8, device="cuda")
+    with pytest.raises(hsi.HsiError) as e:
+        hsi.detect(s, None, 8, 8, 0.1, 0, 0, 16, workspace=small)
+    assert e.value.status == hsi.E_WORKSPACE
