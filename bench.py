@@ -214,7 +214,7 @@ class ClockSampler:
                 sm.append(float(r[1]))
                 mx = float(r[2])
                 for i, n in enumerate(names):
-                    if "Active" in r[5 + i]:
+                    if r[5 + i].strip() == "Active":
                         reasons.add(n)
             except (ValueError, IndexError):
                 continue

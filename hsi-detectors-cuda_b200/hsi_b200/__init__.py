@@ -113,7 +113,10 @@ def _optional_symbols(L):
     table = {
         "hsi_stats_workspace_bytes": ([i32, i32, i32], C.c_size_t),
         "hsi_scene_moments": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
-        "hsi_build_statistics": ([vp, vp, f64, i32, vp, vp, i32, f64, vp, vp, vp, vp, vp, vp, vp], i32),
+        "hsi_scene_moments_simt": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
+        "hsi_statistics_elements": ([i32, i32], C.c_size_t),
+        "hsi_factor_workspace_bytes": ([i32, i32], C.c_size_t),
+        "hsi_build_statistics": ([i32, i32, i32, f64, vp, vp, i64, vp, vp, vp, vp, vp, C.c_size_t, vp], i32),
         "hsi_rx_ace": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, vp, i32, vp, vp, vp, vp, i64, vp], i32),
         "hsi_rx_ace_simt": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, vp, i32, vp, vp, vp, vp, i64, vp], i32),
         "hsi_demosaic": ([vp, i32, i32, i32, i32, vp, vp, i64, vp], i32),
@@ -283,3 +286,84 @@ def detections_to_numpy(count, out, capacity):
     raw = out[:k].cpu().numpy()
     dt = np.dtype([("x", "<i4"), ("y", "<i4"), ("target", "<i4"), ("score", "<f4")])
     return n, raw.view(dt).reshape(-1) if k > 0 else np.zeros(0, dt)
+
+
+# ---------------------------------------------------------------------------
+# scene statistics and FP64 factorisation
+# ---------------------------------------------------------------------------
+
+E_CORRELATION_NOT_PD = 10006
+E_EMPTY = 10007
+
+
+def stats_workspace_bytes(height, width, bands) -> int:
+    return lib().hsi_stats_workspace_bytes(height, width, bands)
+
+
+def moments_elements(bands) -> int:
+    return bands + bands * bands + 1
+
+
+def scene_moments(cube, height, width, bands, dtype=F32, stride=None, out=None, reference=None, workspace=None,
+                  simt=False, stream=None):
+    """Raw moments of one frame on the device: (B + B*B + 1,) float64 = sum, outer, count
+    (the reference's SpectralMoments).  simt=True uses the plain FP32 CUDA-core path."""
+    torch = _torch()
+    dev = cube.device
+    stride = cube.shape[-1] if stride is None else stride
+    if out is None:
+        out = torch.empty(moments_elements(bands), dtype=torch.float64, device=dev)
+    if workspace is None:
+        workspace = torch.empty(stats_workspace_bytes(height, width, bands), dtype=torch.uint8, device=dev)
+    fn = lib().hsi_scene_moments_simt if simt else lib().hsi_scene_moments
+    check(fn(_ptr(cube), height, width, bands, dtype, stride, _ptr(out), _ptr(reference), _ptr(workspace),
+             workspace.numel(), _stream(stream)), "hsi_scene_moments")
+    return out
+
+
+def split_moments(m, bands):
+    """(sum, outer, count) views of a moments vector."""
+    return m[:bands], m[bands:bands + bands * bands].reshape(bands, bands), m[bands + bands * bands]
+
+
+def statistics_elements(bands, targets) -> int:
+    return lib().hsi_statistics_elements(bands, targets)
+
+
+def unpack_statistics(flat, bands, targets):
+    """Packed statistics -> dict (mean, whitener, target_white, target_norm2, cem_weight)."""
+    B, T = bands, targets
+    o = 0
+    out = {}
+    for name, n, shape in (("mean", B, (B,)), ("whitener", B * B, (B, B)), ("target_white", T * B, (T, B)),
+                           ("target_norm2", T, (T,)), ("cem_weight", T * B, (T, B))):
+        out[name] = flat[o:o + n].reshape(shape)
+        o += n
+    return out
+
+
+def build_statistics(moments, bands, library=None, loading=1e-6, want64=True, want32=False, cem_weights=None,
+                     status=None, library_stride=0, stream=None):
+    """FP64 detector statistics on the device for a batch of frames.
+
+    moments: (F, B+B*B+1) or (B+B*B+1,) float64 device tensor.  library: (T, B) shared or
+    (F, T, B) per-frame float32 device tensor.  Returns (stats64 (F, n) or None,
+    stats32 (F, n) or None, status (F,) int32)."""
+    torch = _torch()
+    dev = moments.device
+    m = moments.reshape(-1, moments_elements(bands))
+    F = m.shape[0]
+    T = 0 if library is None else library.shape[-2]
+    if library is not None and library.dim() == 3:
+        library_stride = library.shape[1] * library.shape[2]
+    n = statistics_elements(bands, T)
+    s64 = torch.zeros((F, n), dtype=torch.float64, device=dev) if want64 else None
+    s32 = torch.zeros((F, n), dtype=torch.float32, device=dev) if want32 else None
+    if status is None:
+        status = torch.full((F,), -1, dtype=torch.int32, device=dev)
+    wsb = lib().hsi_factor_workspace_bytes(F, bands)
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+    check(lib().hsi_build_statistics(F, bands, T, float(loading), _ptr(m), _ptr(library), library_stride,
+                                     _ptr(s64), _ptr(s32), _ptr(cem_weights), _ptr(status), _ptr(ws), wsb,
+                                     _stream(stream)), "hsi_build_statistics")
+    return s64, s32, status

@@ -41,11 +41,13 @@ typedef struct CUstream_st* hsi_stream_t;
 /* ---- status codes -------------------------------------------------------- */
 #define HSI_OK 0
 #define HSI_E_INVALID 1             /* == cudaErrorInvalidValue */
-#define HSI_E_NOT_POSITIVE_DEFINITE 10001
+#define HSI_E_NOT_POSITIVE_DEFINITE 10001 /* the scene covariance failed to factor */
 #define HSI_E_TIMEOUT 10002         /* a bounded device-side wait gave up */
 #define HSI_E_WORKSPACE 10003       /* workspace missing or too small */
 #define HSI_E_CAPACITY 10004        /* a size exceeds a documented maximum */
 #define HSI_E_NO_DEVICE 10005
+#define HSI_E_CORRELATION_NOT_PD 10006 /* the CEM autocorrelation failed to factor */
+#define HSI_E_EMPTY 10007              /* no pixels accumulated */
 
 /* ---- element types of a cube --------------------------------------------- */
 #define HSI_F32 0
@@ -170,6 +172,53 @@ HSI_API int hsi_score_frames(const hsi_frame* frames, int num_frames, hsi_stream
 #define HSI_MAX_TABLE_FRAMES 256
 HSI_API int hsi_score_frames_device(const hsi_frame* d_frames, int num_frames, int dtype, int max_bands,
                                     int max_sam, int max_cem, int* d_status, hsi_stream_t stream);
+
+/* ---- scene statistics -------------------------------------------------------
+ * Raw first and second moments of one frame, on the tensor cores: sums about a
+ * per-band reference r (near the mean) split into BF16 hi/lo parts, FP32
+ * accumulation in TMEM over 1024-pixel chunks folded into FP64, then rebuilt
+ * as raw moments in FP64.  Output `d_moments` (FP64): sum[B], outer[B*B]
+ * (full symmetric), count -- the contents of hsi::SpectralMoments.  Replaces
+ * the reference's launch_reset_moments / launch_accumulate_mean /
+ * launch_accumulate_moments / read_moments (include/hsi/stats_cuda.hpp:26-72,
+ * src/stats.cu:169-248) and accumulate_moments_cpu
+ * (src/detectors_cpu.cpp:77-93).  `d_reference` (nullable, `bands` floats):
+ * the shift, e.g. the previous frame's mean; null samples the frame.
+ * Tensor-core path for bands <= 127; 128..256 bands use the FP32 SIMT path.
+ */
+HSI_API size_t hsi_stats_workspace_bytes(int height, int width, int bands);
+HSI_API int hsi_scene_moments(const void* d_cube, int height, int width, int bands, int dtype,
+                              int64_t plane_stride, double* d_moments, const float* d_reference,
+                              void* d_workspace, size_t workspace_bytes, hsi_stream_t stream);
+/* Same moments with plain FP32 CUDA-core arithmetic (register-blocked, FP32
+ * chunks folded into FP64): the comparator for the tensor-core path. */
+HSI_API int hsi_scene_moments_simt(const void* d_cube, int height, int width, int bands, int dtype,
+                                   int64_t plane_stride, double* d_moments, const float* d_reference,
+                                   void* d_workspace, size_t workspace_bytes, hsi_stream_t stream);
+
+/* ---- detector statistics (FP64 factorisation) --------------------------------
+ * For each of `num_frames` frames (moments contiguous, B + B*B + 1 doubles
+ * each) build the statistics of reference build_statistics
+ * (src/detector.cpp:47-152, include/hsi/detector.hpp:62-99) entirely in FP64
+ * on the device: Cholesky of the loaded covariance and autocorrelation,
+ * triangular inverse, whitened targets, CEM weights.  Packed layout per frame
+ * (elements; hsi_statistics_elements gives the total):
+ *   mean[B] | whitener[B*B] (row-major, upper zero) | target_white[T*B] |
+ *   target_norm2[T] | cem_weight[T*B]
+ * `d_stats64` receives it in FP64, `d_stats32` narrowed to float (the
+ * reference's DetectorStatistics), `d_cem_weights` just the CEM filters
+ * (T*B floats per frame) for the scorer; each nullable.  `d_library`: T*B
+ * floats per frame at `library_stride` (0: one library for all frames).
+ * `d_status[f]` (nullable) receives HSI_OK, HSI_E_NOT_POSITIVE_DEFINITE,
+ * HSI_E_CORRELATION_NOT_PD or HSI_E_EMPTY.  Bands > 128 need a workspace of
+ * hsi_factor_workspace_bytes.
+ */
+HSI_API size_t hsi_statistics_elements(int bands, int num_targets);
+HSI_API size_t hsi_factor_workspace_bytes(int num_frames, int bands);
+HSI_API int hsi_build_statistics(int num_frames, int bands, int num_targets, double loading,
+                                 const double* d_moments, const float* d_library, int64_t library_stride,
+                                 double* d_stats64, float* d_stats32, float* d_cem_weights, int* d_status,
+                                 void* d_workspace, size_t workspace_bytes, hsi_stream_t stream);
 
 /* ---- detection compaction ---------------------------------------------------
  * Threshold + non-maximum suppression + compaction of one score map into a
