@@ -62,7 +62,7 @@ def parse():
 
 
 # Both arms (ours and --impl reference) run this workload unless told otherwise.
-DEFAULT_WORKLOAD = "sam"
+DEFAULT_WORKLOAD = "sam_cem"
 
 
 # ---------------------------------------------------------------------------
@@ -256,8 +256,9 @@ class Workload:
             self.cem_best = torch.empty((frames, P), device=device)
             self.cem_bt = torch.empty((frames, P), dtype=torch.int32, device=device)
             self.stats_bytes = hsi.lib().hsi_stats_workspace_bytes(H, W, B)
-            self.stats_ws = torch.empty((frames, self.stats_bytes), dtype=torch.uint8, device=device)
+            self.stats_ws = torch.empty(self.stats_bytes, dtype=torch.uint8, device=device)
             self.moments = torch.zeros((frames, B + B * B + 1), dtype=torch.float64, device=device)
+            self.status = torch.zeros(frames, dtype=torch.int32, device=device)
         self.table = self._table(self.cubes)
         self.launches_per_step = 0
 
@@ -280,19 +281,21 @@ class Workload:
         launches = 0
         L = hsi.lib()
         s = C.c_void_p(stream.cuda_stream)
+        if events is not None:
+            events[2].record(stream)
         if self.cem:
             for f in range(self.n):
                 hsi.check(L.hsi_scene_moments(C.c_void_p(self.cubes[f].data_ptr()), H, W, B, 0, self.stride,
                                               C.c_void_p(self.moments[f].data_ptr()), None,
-                                              C.c_void_p(self.stats_ws[f].data_ptr()), self.stats_bytes, s),
+                                              C.c_void_p(self.stats_ws.data_ptr()), self.stats_bytes, s),
                           "hsi_scene_moments")
                 launches += self.stats_launches
-            for f in range(self.n):
-                hsi.check(L.hsi_build_statistics(
-                    C.c_void_p(self.moments[f].data_ptr()), None, 0.0, B, C.c_void_p(self.targets.data_ptr()),
-                    None, TARGETS, LOADING, None, None, None, None, C.c_void_p(self.cem_w[f].data_ptr()),
-                    C.c_void_p(self.stats_ws[f].data_ptr()), s), "hsi_build_statistics")
-                launches += self.factor_launches
+            # one launch factors every frame (one CTA per frame, FP64)
+            hsi.check(L.hsi_build_statistics(self.n, B, TARGETS, LOADING, C.c_void_p(self.moments.data_ptr()),
+                                             C.c_void_p(self.targets.data_ptr()), 0, None, None,
+                                             C.c_void_p(self.cem_w.data_ptr()), C.c_void_p(self.status.data_ptr()),
+                                             None, 0, s), "hsi_build_statistics")
+            launches += 1
         if events is not None:
             events[0].record(stream)
         hsi.score_frames_device(self.table, self.n, B, TARGETS, TARGETS if self.cem else 0, stream=stream)
@@ -306,8 +309,8 @@ class Workload:
             launches += 3
         return launches
 
-    stats_launches = 2
-    factor_launches = 1
+    # shift, GEMM, conditional rescale + re-run, reduce, finalize
+    stats_launches = 6
 
 
 def algorithmic_bytes_score(frames, cem):
@@ -360,7 +363,7 @@ def run_ours(args, workload):
     uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else (str(uuid) if uuid else None)
 
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(args.steps)]
     barrier()
     torch.cuda.synchronize()
     launches = 0
@@ -372,11 +375,12 @@ def run_ours(args, workload):
         torch.cuda.synchronize()
     barrier()
     ms = start.elapsed_time(end) / args.steps
-    kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in kev]))
+    kernel_ms = float(np.mean([a.elapsed_time(b) for a, b, _ in kev]))
+    stats_ms = float(np.mean([c.elapsed_time(a) for a, _, c in kev]))
     if world > 1:
-        t = torch.tensor([ms, kernel_ms], device=device, dtype=torch.float64)
+        t = torch.tensor([ms, kernel_ms, stats_ms], device=device, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, kernel_ms = float(t[0]), float(t[1])
+        ms, kernel_ms, stats_ms = float(t[0]), float(t[1]), float(t[2])
     pixels_step = args.frames * H * W
     value = world * pixels_step / (ms / 1e3) / 1e6
 
@@ -395,6 +399,13 @@ def run_ours(args, workload):
                 "traffic": traffic, "kernel_ms": round(kernel_ms, 3),
                 "algorithmic_bytes_per_launch": algorithmic_bytes_score(args.frames, wl.cem)}
     step_bytes = algorithmic_bytes_step(args.frames, wl.cem)
+    roofline_stats = None
+    if wl.cem:
+        sb = args.frames * H * W * 4 * B
+        ach = sb / (stats_ms / 1e3) / 1e9
+        roofline_stats = {"kernel": "scene moments (INT8-limb tcgen05 GEMM) + FP64 factor, all frames",
+                          "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                          "frac": round(ach / hbm, 4), "ms": round(stats_ms, 3), "algorithmic_bytes": sb}
 
     e2e = None
     if not args.no_e2e:
@@ -418,6 +429,7 @@ def run_ours(args, workload):
             "data": "synthetic (seeded scene model generated on the device)",
             "config": dict(workload_config(workload, args.frames), parallelism=f"frames sharded over {world} GPU(s)"),
             "roofline": roofline,
+            "roofline_stats": roofline_stats,
             "step_hbm_fraction": round(step_bytes / (ms / 1e3) / 1e9 / hbm, 4),
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
         }
@@ -474,12 +486,12 @@ def run_e2e(hsi, torch, wl, stream, args, world):
             if wl.cem:
                 hsi.check(L.hsi_scene_moments(C.c_void_p(dev[i].data_ptr()), H, W, B, 0, wl.stride,
                                               C.c_void_p(wl.moments[i].data_ptr()), None,
-                                              C.c_void_p(wl.stats_ws[i].data_ptr()), wl.stats_bytes, s), "moments")
-                hsi.check(L.hsi_build_statistics(
-                    C.c_void_p(wl.moments[i].data_ptr()), None, 0.0, B, C.c_void_p(wl.targets.data_ptr()), None,
-                    TARGETS, LOADING, None, None, None, None, C.c_void_p(wl.cem_w[i].data_ptr()),
-                    C.c_void_p(wl.stats_ws[i].data_ptr()), s), "stats")
-                launches += wl.stats_launches + wl.factor_launches
+                                              C.c_void_p(wl.stats_ws.data_ptr()), wl.stats_bytes, s), "moments")
+                hsi.check(L.hsi_build_statistics(1, B, TARGETS, LOADING, C.c_void_p(wl.moments[i].data_ptr()),
+                                                 C.c_void_p(wl.targets.data_ptr()), 0, None, None,
+                                                 C.c_void_p(wl.cem_w[i].data_ptr()),
+                                                 C.c_void_p(wl.status[i:i + 1].data_ptr()), None, 0, s), "stats")
+                launches += wl.stats_launches + 1
             hsi.score_frames([frames[i]], stream=stream)
             freed[i].record(stream)
             wl.counts[f:f + 1].zero_()

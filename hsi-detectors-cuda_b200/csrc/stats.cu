@@ -1,32 +1,42 @@
-// stats.cu - scene moments on the 5th-generation tensor cores.
+// stats.cu - scene moments on the 5th-generation tensor cores, exactly.
 //
 // Computes, for one BSQ frame, the raw first and second moments the detector
 // statistics are built from (reference: SpectralMoments, include/hsi/linalg.hpp
 // :22-51, accumulated by src/detectors_cpu.cpp:77-93 on the CPU and by the
 // never-called src/stats.cu:72-165 on the GPU).
 //
-// Arithmetic (precision measured against the FP64 oracle before writing it):
-//   d = x - r, r a per-band reference near the mean (the reference's shifted
-//   accumulation, include/hsi/linalg.hpp:53-90);
-//   d is split into BF16 hi + lo, H = bf16(d), L = bf16(d - H), and the tensor
-//   cores accumulate  G' = H H^T + L L^T + H (2L)^T  (three MMAs per K-step),
-//   so that S = (G' + G'^T)/2 = H H^T + L L^T + H L^T + L H^T -- all four
-//   products, because dropping L L^T biases the variances;
-//   a ones-row at band B makes the same GEMM produce sum(d) and the pixel count;
-//   FP32 accumulation in TMEM is limited to 1024-pixel chunks, each folded into
-//   an FP64 accumulator that also lives in TMEM (the reference's FP32-block ->
-//   FP64 hierarchy, tests/test_linalg.cpp:290-350);
-//   partial sums of all CTAs are reduced in a fixed order (deterministic), and
-//   the raw moments are rebuilt in FP64 (src/linalg.cpp:81-103).
+// Why integers.  RX/ACE amplify relative covariance errors by the condition
+// number of the (loaded) covariance, ~4000 for these scenes, so 1e-4 on the
+// scores needs the second moments to ~2e-8.  Measured on B200, FP32
+// accumulation on the tensor cores truncates: BF16 hi/lo products with all four
+// terms still left a 5e-7..5e-6 bias (RX error 5e-4..3e-3), and even FP32
+// CUDA-core FMAs over 1024-pixel chunks gave 1.8e-4.  Integer MMAs accumulate
+// exactly.  So:
+//   d = x - r (r: per-band reference near the mean, as the reference's shifted
+//   accumulation, include/hsi/linalg.hpp:53-90), fixed point
+//   q = rint(d * 2^e_b) with |q| < 2^23 (e_b from a subsample with 4x headroom;
+//   an overflow re-runs the pass with the observed range), balanced signed
+//   8-bit limbs q = L0*2^16 + L1*2^8 + L2, and four exact INT32 accumulators
+//     A0 = sum L0 L0^T,  A1 = sum L0 L1^T,  A2 = sum (L1 L1^T + 2 L0 L2^T),
+//     A3 = sum 2 L1 L2^T
+//   (tcgen05.mma kind::i8, seven MMAs per K-step).  F = 2^32 A0 + 2^25 A1 +
+//   2^16 A2 + 2^8 A3 in FP64 and S = (F + F^T)/2 is sum q q^T except the
+//   weight-1 products L2 L2^T: their diagonal is added back exactly (the
+//   converters count sum L2^2 per band), their off-diagonal sums are those of
+//   independent rounding residues.  The cross terms matter: when outliers set
+//   the fixed-point range, typical q carry only ~15 significant bits.
+//   A ones-row at band B (q = 2^16) makes the same GEMM produce sum(q) and the
+//   pixel count.  Partial sums of all CTAs are reduced in a fixed order and
+//   rebuilt as raw moments in FP64 (src/linalg.cpp:81-103).
 //
 // Kernel roles (one CTA per SM, 14 warps):
-//   warp 0       TMA producer: 2-D tiles of 64 pixels x 128 bands
+//   warp 0       TMA producer: two 64-pixel x 128-band boxes per K-block
 //   warp 1       TMEM allocator + single-thread MMA issuer
-//   warps 2-9    converters: FP32 tile -> BF16 H, L, 2L in the UMMA
-//                128-byte-swizzled K-major layout
-//   warps 10-13  epilogue: TMEM chunk -> FP64 TMEM accumulator -> global
-// TMEM: columns [0,128) and [128,256) double-buffer the FP32 chunk
-// accumulator; [256,512) hold the FP64 accumulator (two columns per value).
+//   warps 2-9    converters: FP32 tile -> INT8 limbs L0, L1, L2 in the UMMA
+//                128-byte-swizzled K-major layout; per-band |d| maxima
+//   warps 10-13  epilogue: INT32 TMEM accumulators -> FP64 partials (once per
+//                32768-pixel chunk, i.e. once per frame at typical sizes)
+// TMEM: columns [0,128) A0, [128,256) A1, [256,384) A2, [384,512) A3.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -35,13 +45,10 @@
 namespace hsi_b200 {
 namespace {
 
-constexpr int kKB = 64;          // pixels per K-block (one TMA box)
-#ifndef HSI_STATS_CHUNK_KB
-#define HSI_STATS_CHUNK_KB 16
-#endif
-constexpr int kChunkKB = HSI_STATS_CHUNK_KB;  // K-blocks per FP32 accumulation chunk
+constexpr int kKB = 128;         // pixels per K-block (one INT8 operand row)
+constexpr int kBoxPx = 64;       // pixels per TMA box
+constexpr int kChunkKB = 256;    // K-blocks per INT32 chunk: 32768 px, no overflow
 constexpr int kRows = 128;       // band rows of the GEMM (bands + ones row)
-constexpr int kInStages = 3;
 constexpr int kOpStages = 2;
 constexpr int kConvWarps = 8;
 constexpr int kEpiWarps = 4;
@@ -50,19 +57,25 @@ constexpr int kWarpMma = 1;
 constexpr int kWarpConv0 = 2;
 constexpr int kWarpEpi0 = kWarpConv0 + kConvWarps;
 constexpr int kThreads = (kWarpEpi0 + kEpiWarps) * 32;  // 448
-constexpr int kOpTileBytes = kRows * kKB * 2;           // 16 KB (BF16)
+constexpr int kLimbBytes = kRows * kKB;                 // 16 KB per limb tile
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kFp64Col = 256;
 constexpr int kMaxTensorBands = kRows - 1;  // 127: room for the ones row
 constexpr int kMaxCtas = 160;
+constexpr int64_t kTensorMinPixels = 32768;
+constexpr int kQMax = (1 << 23) - (1 << 16) - 1;
+constexpr int kOnesExp = 16;  // the ones row holds q = 2^16
 
+template <typename T>
+constexpr int in_stages() {
+  return sizeof(T) == 4 ? 2 : 4;
+}
 template <typename T>
 constexpr int in_tile_bytes() {
   return kRows * kKB * static_cast<int>(sizeof(T));
 }
 
 struct StatsSmem {
-  size_t in_off, op_off, shift_off, bar_off, slot_off, total;
+  size_t in_off, op_off, shift_off, scale_off, bar_off, slot_off, total;
 };
 
 template <typename T>
@@ -70,64 +83,94 @@ __host__ __device__ inline StatsSmem stats_smem() {
   StatsSmem s;
   size_t off = 0;
   s.in_off = off;
-  off += static_cast<size_t>(kInStages) * in_tile_bytes<T>();
+  off += static_cast<size_t>(in_stages<T>()) * in_tile_bytes<T>();
   s.op_off = off;  // 1024-aligned: in tiles are multiples of 1024
-  off += static_cast<size_t>(kOpStages) * 3 * kOpTileBytes;
+  off += static_cast<size_t>(kOpStages) * 3 * kLimbBytes;
   s.shift_off = off;
   off += kRows * sizeof(float);
+  s.scale_off = off;
+  off += kRows * sizeof(float);
   s.bar_off = off;
-  off += (2 * kInStages + 2 * kOpStages + 5) * sizeof(uint64_t);
+  off += (2 * 4 + 2 * kOpStages + 3) * sizeof(uint64_t);
   s.slot_off = off;
   off += 16;
   s.total = off + 1024;  // slack to align the dynamic base to 1024
   return s;
 }
 
-// Byte offset of element (row, k) in a 128B-swizzled K-major tile of 16-bit
-// values with 64 elements per row.
-__device__ __forceinline__ uint32_t sw128_offset(int row, int k) {
-  const int chunk = (k * 2) >> 4;
-  return static_cast<uint32_t>((row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4) + ((k * 2) & 15));
+// Byte offset of byte k of row `row` in a 128B-swizzled K-major tile whose rows
+// are 128 bytes (8-row atoms of 1024 bytes).
+__device__ __forceinline__ uint32_t sw128_byte(int row, int k) {
+  return static_cast<uint32_t>((row >> 3) * 1024 + (row & 7) * 128 + ((((k >> 4) ^ (row & 7))) << 4) + (k & 15));
 }
 
 template <typename T>
-__device__ __forceinline__ float2 load_pair(const T* p);
+__device__ __forceinline__ float4 load4f(const T* p);
 template <>
-__device__ __forceinline__ float2 load_pair<float>(const float* p) {
-  return *reinterpret_cast<const float2*>(p);
+__device__ __forceinline__ float4 load4f<float>(const float* p) {
+  return *reinterpret_cast<const float4*>(p);
 }
 template <>
-__device__ __forceinline__ float2 load_pair<__half>(const __half* p) {
-  return __half22float2(*reinterpret_cast<const __half2*>(p));
+__device__ __forceinline__ float4 load4f<__half>(const __half* p) {
+  const uint2 raw = *reinterpret_cast<const uint2*>(p);
+  const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+  const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+  return make_float4(a.x, a.y, b.x, b.y);
 }
 
-__device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
+// Workspace shared by the launch sequence of one frame.
+struct StatsState {
+  float shift[HSI_MAX_BANDS + 1];     // r_b
+  int scale_exp[HSI_MAX_BANDS + 1];   // e_b (ones row: kOnesExp)
+  int maxdev_bits[HSI_MAX_BANDS + 1]; // max |d_b| seen by the GEMM (float bits, >= 0)
+  int flags;                          // bit 0: a q was clamped; bit 1: the re-run is armed
+  int pad[3];
+  unsigned long long l2sq[HSI_MAX_BANDS + 1];  // exact sum of L2^2 per band
+};
 
 struct StatsArgs {
   int64_t pixels;
   int bands;
-  const float* shift;  // kRows floats (0 past the bands)
-  double* partials;    // [gridDim.x][kRows][kRows] (column-major per CTA)
+  StatsState* state;
+  double* partials;  // [gridDim.x][kRows][kRows] (column-major per CTA)
+  int conditional;   // 1: run only if the re-run is armed
   int* status;
 };
+
+// Split q (|q| <= kQMax) into balanced signed bytes: q = l0*2^16 + l1*2^8 + l2.
+__device__ __forceinline__ void limbs(int q, int& l0, int& l1, int& l2) {
+  l2 = ((q + 128) & 255) - 128;
+  const int q1 = (q - l2) >> 8;
+  l1 = ((q1 + 128) & 255) - 128;
+  l0 = (q1 - l1) >> 8;
+}
+
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
+  return (static_cast<uint32_t>(a) & 255u) | ((static_cast<uint32_t>(b) & 255u) << 8) |
+         ((static_cast<uint32_t>(c) & 255u) << 16) | ((static_cast<uint32_t>(d) & 255u) << 24);
+}
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 1)
     stats_gemm_kernel(const __grid_constant__ CUtensorMap cube_map, const StatsArgs args) {
+  if (args.conditional && !(args.state->flags & 2)) return;  // nothing to redo
+  constexpr int kInStages = in_stages<T>();
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const StatsSmem L = stats_smem<T>();
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
   uint64_t* in_full = bars;
-  uint64_t* in_empty = in_full + kInStages;
-  uint64_t* op_full = in_empty + kInStages;
+  uint64_t* in_empty = in_full + 4;
+  uint64_t* op_full = in_empty + 4;
   uint64_t* op_empty = op_full + kOpStages;
   uint64_t* acc_full = op_empty + kOpStages;
-  uint64_t* acc_empty = acc_full + 2;
-  uint64_t* mma_done = acc_empty + 2;
+  uint64_t* acc_empty = acc_full + 1;
+  uint64_t* mma_done = acc_empty + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.slot_off);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.slot_off + 8);
+  int* clamp_flag = reinterpret_cast<int*>(smem + L.slot_off + 12);
   float* shift = reinterpret_cast<float*>(smem + L.shift_off);
+  float* scale = reinterpret_cast<float*>(smem + L.scale_off);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t P = args.pixels;
@@ -147,15 +190,17 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&op_full[s], kConvWarps);
       mbar_init(&op_empty[s], 1);
     }
-    for (int s = 0; s < 2; ++s) {
-      mbar_init(&acc_full[s], 1);
-      mbar_init(&acc_empty[s], kEpiWarps);
-    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, kEpiWarps);
     mbar_init(mma_done, 1);
     *abort_flag = 0;
+    *clamp_flag = 0;
     fence_barrier_init();
   }
-  for (int i = threadIdx.x; i < kRows; i += blockDim.x) shift[i] = args.shift[i];
+  for (int i = threadIdx.x; i < kRows; i += blockDim.x) {
+    shift[i] = args.state->shift[i];
+    scale[i] = ldexpf(1.0f, args.state->scale_exp[i]);
+  }
   if (warp == kWarpMma) tmem_alloc(tmem_slot, kTmemCols);
   tc_fence_before();
   __syncthreads();
@@ -174,9 +219,11 @@ __global__ void __launch_bounds__(kThreads, 1)
           *abort_flag = 1;
           break;
         }
+        unsigned char* dst = smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>();
         mbar_arrive_expect_tx(&in_full[s], in_tile_bytes<T>());
-        tma_load_2d(smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>(), &cube_map,
-                    static_cast<int>((kb0 + i) * kKB), 0, &in_full[s]);
+        const int x = static_cast<int>((kb0 + i) * kKB);
+        tma_load_2d(dst, &cube_map, x, 0, &in_full[s]);
+        tma_load_2d(dst + in_tile_bytes<T>() / 2, &cube_map, x + kBoxPx, 0, &in_full[s]);
         pending |= 1u << s;
         parity = (parity & ~(1u << s)) | (ph << s);
       }
@@ -185,13 +232,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == kWarpMma) {
     if (lane == 0) {
-      const uint32_t idesc = idesc_bf16_f32(kRows, kRows);
+      const uint32_t idesc = idesc_s8_s32(kRows, kRows);
       bool issued = false;
       for (int i = 0; i < n && !*abort_flag; ++i) {
         const int chunk = i / kChunkKB, j = i % kChunkKB;
-        const int buf = chunk & 1;
         if (j == 0) {
-          if (!mbar_wait(&acc_empty[buf], ((chunk >> 1) & 1u) ^ 1u)) {
+          if (!mbar_wait(acc_empty, (chunk & 1u) ^ 1u)) {
             record_error(args.status, HSI_E_TIMEOUT);
             *abort_flag = 1;
             break;
@@ -205,20 +251,24 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         tc_fence_after();
-        unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kOpTileBytes;
-        const uint64_t dH = smem_desc_sw128(op);
-        const uint64_t dL = smem_desc_sw128(op + kOpTileBytes);
-        const uint64_t dL2 = smem_desc_sw128(op + 2 * kOpTileBytes);
-        const uint32_t d = tmem + static_cast<uint32_t>(buf * kRows);
+        unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kLimbBytes;
+        const uint64_t d0 = smem_desc_sw128(op);
+        const uint64_t d1 = smem_desc_sw128(op + kLimbBytes);
+        const uint64_t d2 = smem_desc_sw128(op + 2 * kLimbBytes);
 #pragma unroll
-        for (int k = 0; k < kKB / 16; ++k) {
+        for (int k = 0; k < kKB / 32; ++k) {
           const uint64_t adv = static_cast<uint64_t>(k * 2);  // 32 bytes of K, in 16-byte units
-          umma_f16(d, dH + adv, dH + adv, idesc, (j > 0 || k > 0) ? 1u : 0u);
-          umma_f16(d, dL + adv, dL + adv, idesc, 1u);
-          umma_f16(d, dH + adv, dL2 + adv, idesc, 1u);
+          const uint32_t acc = (j > 0 || k > 0) ? 1u : 0u;
+          umma_i8(tmem + 0, d0 + adv, d0 + adv, idesc, acc);
+          umma_i8(tmem + 128, d0 + adv, d1 + adv, idesc, acc);
+          umma_i8(tmem + 256, d1 + adv, d1 + adv, idesc, acc);
+          umma_i8(tmem + 256, d0 + adv, d2 + adv, idesc, 1u);
+          umma_i8(tmem + 256, d0 + adv, d2 + adv, idesc, 1u);
+          umma_i8(tmem + 384, d1 + adv, d2 + adv, idesc, acc);
+          umma_i8(tmem + 384, d1 + adv, d2 + adv, idesc, 1u);
         }
         umma_commit(&op_empty[so]);
-        if (j == kChunkKB - 1 || i == n - 1) umma_commit(&acc_full[buf]);
+        if (j == kChunkKB - 1 || i == n - 1) umma_commit(acc_full);
         issued = true;
       }
       // TMEM is freed at the end of the kernel: make sure no MMA of this
@@ -230,11 +280,20 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp < kWarpEpi0) {
     // ---------------- converters ----------------
+    // warp cw: bands cw + 8t (t < 16); lane: pixels 4*lane .. 4*lane + 3
     const int cw = warp - kWarpConv0;
-    float rr[kRows / kConvWarps];
+    constexpr int kBandsPerWarp = kRows / kConvWarps;
+    float rr[kBandsPerWarp], sc[kBandsPerWarp], mx[kBandsPerWarp];
+    uint32_t l2sq[kBandsPerWarp];
 #pragma unroll
-    for (int t = 0; t < kRows / kConvWarps; ++t) rr[t] = shift[cw + kConvWarps * t];
-    bool aborted = false;
+    for (int t = 0; t < kBandsPerWarp; ++t) {
+      rr[t] = shift[cw + kConvWarps * t];
+      sc[t] = scale[cw + kConvWarps * t];
+      mx[t] = 0.0f;
+      l2sq[t] = 0u;
+    }
+    bool aborted = false, clamped = false;
+    const int half = lane >> 4, hp = (lane & 15) * 4;  // box half and pixel within it
     for (int i = 0; i < n; ++i) {
       const int s = i % kInStages, so = i % kOpStages;
       if (!aborted && (!mbar_wait(&in_full[s], (i / kInStages) & 1u) ||
@@ -244,31 +303,45 @@ __global__ void __launch_bounds__(kThreads, 1)
         aborted = true;
       }
       if (aborted) break;
-      const T* in = reinterpret_cast<const T*>(smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>());
-      unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kOpTileBytes;
-      const int64_t gp = (kb0 + i) * kKB + 2 * lane;
-      const bool v0 = gp < P, v1 = gp + 1 < P;
+      const T* in = reinterpret_cast<const T*>(smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>()) +
+                    half * (kRows * kBoxPx);
+      unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kLimbBytes;
+      const int64_t gp = (kb0 + i) * kKB + 4 * lane;
+      const int nvalid = gp >= P ? 0 : (P - gp >= 4 ? 4 : static_cast<int>(P - gp));
 #pragma unroll
-      for (int t = 0; t < kRows / kConvWarps; ++t) {
+      for (int t = 0; t < kBandsPerWarp; ++t) {
         const int b = cw + kConvWarps * t;
-        float d0 = 0.0f, d1 = 0.0f;
+        int q[4] = {0, 0, 0, 0};
         if (b < B) {
-          const float2 x = load_pair<T>(in + b * kKB + 2 * lane);
-          d0 = v0 ? x.x - rr[t] : 0.0f;
-          d1 = v1 ? x.y - rr[t] : 0.0f;
+          const float4 x = load4f<T>(in + b * kBoxPx + hp);
+          const float xv[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            if (e < nvalid) {
+              const float d = xv[e] - rr[t];
+              mx[t] = fmaxf(mx[t], fabsf(d));
+              int v = __float2int_rn(d * sc[t]);
+              if (v > kQMax || v < -kQMax || !(fabsf(d * sc[t]) <= static_cast<float>(kQMax))) {
+                clamped = true;
+                v = v > 0 ? kQMax : -kQMax;
+              }
+              q[e] = v;
+            }
+          }
         } else if (b == B) {
-          d0 = v0 ? 1.0f : 0.0f;
-          d1 = v1 ? 1.0f : 0.0f;
+#pragma unroll
+          for (int e = 0; e < 4; ++e) q[e] = e < nvalid ? (1 << kOnesExp) : 0;
         }
-        const __nv_bfloat162 hi = __floats2bfloat162_rn(d0, d1);
-        const float2 hf = __bfloat1622float2(hi);
-        const float r0 = d0 - hf.x, r1 = d1 - hf.y;
-        const __nv_bfloat162 lo = __floats2bfloat162_rn(r0, r1);
-        const __nv_bfloat162 lo2 = __floats2bfloat162_rn(2.0f * r0, 2.0f * r1);
-        const uint32_t off = sw128_offset(b, 2 * lane);
-        *reinterpret_cast<uint32_t*>(op + off) = bf2_bits(hi);
-        *reinterpret_cast<uint32_t*>(op + kOpTileBytes + off) = bf2_bits(lo);
-        *reinterpret_cast<uint32_t*>(op + 2 * kOpTileBytes + off) = bf2_bits(lo2);
+        int l0[4], l1[4], l2[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          limbs(q[e], l0[e], l1[e], l2[e]);
+          l2sq[t] += static_cast<uint32_t>(l2[e] * l2[e]);
+        }
+        const uint32_t off = sw128_byte(b, 4 * lane);
+        *reinterpret_cast<uint32_t*>(op + off) = pack4(l0[0], l0[1], l0[2], l0[3]);
+        *reinterpret_cast<uint32_t*>(op + kLimbBytes + off) = pack4(l1[0], l1[1], l1[2], l1[3]);
+        *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + off) = pack4(l2[0], l2[1], l2[2], l2[3]);
       }
       fence_proxy_async_smem();
       __syncwarp();
@@ -277,71 +350,55 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_arrive(&op_full[so]);
       }
     }
+    // per-band |d| maxima and the clamp flag, for the re-run and for the
+    // whitening pass's fixed-point range
+#pragma unroll
+    for (int t = 0; t < kBandsPerWarp; ++t) {
+      float m = mx[t];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+      const int b = cw + kConvWarps * t;
+      if (lane == 0 && b < B) atomicMax(&args.state->maxdev_bits[b], __float_as_int(m));
+      unsigned long long sq = l2sq[t];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+      if (lane == 0 && b < B) atomicAdd(&args.state->l2sq[b], sq);
+    }
+    if (__any_sync(0xffffffffu, clamped) && lane == 0) atomicOr(&args.state->flags, 1);
   } else {
     // ---------------- epilogue ----------------
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int row = q * 32 + lane;
     const uint32_t trow = tmem + (static_cast<uint32_t>(q * 32) << 16);
-    uint32_t z[32];
-#pragma unroll
-    for (int c = 0; c < 32; ++c) z[c] = 0u;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) tmem_st32(trow + kFp64Col + 32 * c, z);
-    tmem_wait_st();
-    bool aborted = false;
+    double* out = args.partials + static_cast<size_t>(blockIdx.x) * kRows * kRows;
     for (int chunk = 0; chunk < nchunks; ++chunk) {
-      const int buf = chunk & 1;
-      if (!mbar_wait(&acc_full[buf], (chunk >> 1) & 1u)) {
+      if (!mbar_wait(acc_full, chunk & 1u)) {
         record_error(args.status, HSI_E_TIMEOUT);
         *abort_flag = 1;
-        aborted = true;
         break;
       }
       tc_fence_after();
 #pragma unroll 1
-      for (int cb = 0; cb < kRows / 32; ++cb) {
-        uint32_t g[32], f0[32], f1[32];
-        tmem_ld32(trow + buf * kRows + 32 * cb, g);
-        tmem_ld32(trow + kFp64Col + 64 * cb, f0);
-        tmem_ld32(trow + kFp64Col + 64 * cb + 32, f1);
+      for (int cb = 0; cb < kRows / 16; ++cb) {
+        uint32_t a0[16], a1[16], a2[16], a3[16];
+        tmem_ld16(trow + 0 + 16 * cb, a0);
+        tmem_ld16(trow + 128 + 16 * cb, a1);
+        tmem_ld16(trow + 256 + 16 * cb, a2);
+        tmem_ld16(trow + 384 + 16 * cb, a3);
         tmem_wait_ld();
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          double a = __hiloint2double(static_cast<int>(f0[2 * j + 1]), static_cast<int>(f0[2 * j]));
-          a += static_cast<double>(__uint_as_float(g[j]));
-          f0[2 * j] = static_cast<uint32_t>(__double2loint(a));
-          f0[2 * j + 1] = static_cast<uint32_t>(__double2hiint(a));
-          double b = __hiloint2double(static_cast<int>(f1[2 * j + 1]), static_cast<int>(f1[2 * j]));
-          b += static_cast<double>(__uint_as_float(g[16 + j]));
-          f1[2 * j] = static_cast<uint32_t>(__double2loint(b));
-          f1[2 * j + 1] = static_cast<uint32_t>(__double2hiint(b));
+          const double f = ldexp(static_cast<double>(static_cast<int>(a0[j])), 32) +
+                           ldexp(static_cast<double>(static_cast<int>(a1[j])), 25) +
+                           ldexp(static_cast<double>(static_cast<int>(a2[j])), 16) +
+                           ldexp(static_cast<double>(static_cast<int>(a3[j])), 8);
+          double* dst = out + static_cast<size_t>(16 * cb + j) * kRows + row;  // column-major
+          *dst = chunk == 0 ? f : *dst + f;
         }
-        tmem_st32(trow + kFp64Col + 64 * cb, f0);
-        tmem_st32(trow + kFp64Col + 64 * cb + 32, f1);
       }
-      tmem_wait_st();
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&acc_empty[buf]);
-    }
-    if (!aborted && !*abort_flag) {
-      // Column-major per CTA: partial[c][col][row], so a warp's stores of one
-      // column are 32 consecutive doubles.
-      double* out = args.partials + static_cast<size_t>(blockIdx.x) * kRows * kRows;
-#pragma unroll 1
-      for (int cb = 0; cb < kRows / 32; ++cb) {
-        uint32_t f0[32], f1[32];
-        tmem_ld32(trow + kFp64Col + 64 * cb, f0);
-        tmem_ld32(trow + kFp64Col + 64 * cb + 32, f1);
-        tmem_wait_ld();
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          out[static_cast<size_t>(32 * cb + j) * kRows + row] =
-              __hiloint2double(static_cast<int>(f0[2 * j + 1]), static_cast<int>(f0[2 * j]));
-          out[static_cast<size_t>(32 * cb + 16 + j) * kRows + row] =
-              __hiloint2double(static_cast<int>(f1[2 * j + 1]), static_cast<int>(f1[2 * j]));
-        }
-      }
+      if (lane == 0) mbar_arrive(acc_empty);
     }
   }
   tc_fence_before();
@@ -354,45 +411,89 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // ---------------------------------------------------------------------------
-// Shift reference: per-band mean over a regular subsample (every 16th run of
-// 64 pixels), good enough to keep the shifted sums free of cancellation.
+// Reference point and fixed-point scale per band from a regular subsample
+// (every 16th run of 64 pixels on large frames): r = subsample mean, e such
+// that the subsample's largest |x - r| maps to 2^21 (4x headroom below 2^23).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ int scale_exp_for(float maxdev) {
+  if (!(maxdev > 0.0f)) return 21;
+  int e;
+  frexpf(maxdev, &e);  // maxdev in [2^(e-1), 2^e)
+  int k = 21 - e;      // maxdev * 2^k < 2^21
+  return k < -120 ? -120 : (k > 120 ? 120 : k);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) shift_kernel(const T* __restrict__ cube, int64_t pixels, int64_t stride,
-                                                    int bands, const float* __restrict__ given, float* shift) {
+                                                    int bands, const float* __restrict__ given, StatsState* st) {
   const int b = blockIdx.x;
-  if (b >= bands) {
-    if (threadIdx.x == 0) shift[b] = 0.0f;
-    return;
+  if (threadIdx.x == 0) {
+    if (b == 0) st->flags = 0;
+    st->maxdev_bits[b] = 0;
+    st->l2sq[b] = 0ull;
   }
-  if (given) {
-    if (threadIdx.x == 0) shift[b] = given[b];
+  if (b >= bands) {
+    if (threadIdx.x == 0) {
+      st->shift[b] = 0.0f;
+      st->scale_exp[b] = b == bands ? kOnesExp : 0;
+    }
     return;
   }
   __shared__ double s_sum[256];
   __shared__ double s_cnt[256];
+  __shared__ float s_lo[256], s_hi[256];
   const T* plane = cube + static_cast<int64_t>(b) * stride;
   const int64_t runs = div_up<int64_t>(pixels, 64);
   const int64_t step = runs > 4096 ? 16 : 1;
   double sum = 0.0, cnt = 0.0;
+  float lo = INFINITY, hi = -INFINITY;
   for (int64_t run = threadIdx.x / 64; run * step < runs; run += blockDim.x / 64) {
     const int64_t p = run * step * 64 + (threadIdx.x & 63);
     if (p < pixels) {
-      sum += static_cast<double>(static_cast<float>(plane[p]));
+      const float v = static_cast<float>(plane[p]);
+      sum += static_cast<double>(v);
       cnt += 1.0;
+      lo = fminf(lo, v);
+      hi = fmaxf(hi, v);
     }
   }
   s_sum[threadIdx.x] = sum;
   s_cnt[threadIdx.x] = cnt;
+  s_lo[threadIdx.x] = lo;
+  s_hi[threadIdx.x] = hi;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) {
       s_sum[threadIdx.x] += s_sum[threadIdx.x + w];
       s_cnt[threadIdx.x] += s_cnt[threadIdx.x + w];
+      s_lo[threadIdx.x] = fminf(s_lo[threadIdx.x], s_lo[threadIdx.x + w]);
+      s_hi[threadIdx.x] = fmaxf(s_hi[threadIdx.x], s_hi[threadIdx.x + w]);
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) shift[b] = s_cnt[0] > 0.0 ? static_cast<float>(s_sum[0] / s_cnt[0]) : 0.0f;
+  if (threadIdx.x == 0) {
+    float r = given ? given[b] : (s_cnt[0] > 0.0 ? static_cast<float>(s_sum[0] / s_cnt[0]) : 0.0f);
+    const float dev = fmaxf(fabsf(s_hi[0] - r), fabsf(s_lo[0] - r));
+    const int e = scale_exp_for(dev * 1.0000001f);
+    // r on the fixed-point grid: inputs that are themselves multiples of 2^-e
+    // (FP16 cubes, quantised sensors) then convert to q without rounding
+    r = ldexpf(rintf(ldexpf(r, e)), -e);
+    st->shift[b] = r;
+    st->scale_exp[b] = e;
+  }
+}
+
+// After the first GEMM: if a value was clamped, take the range the GEMM
+// actually saw and arm the conditional re-run; otherwise leave it disarmed.
+__global__ void rescale_kernel(int bands, StatsState* st) {
+  if (!(st->flags & 1)) return;
+  for (int b = threadIdx.x; b < bands; b += blockDim.x) {
+    const float dev = __int_as_float(st->maxdev_bits[b]);
+    st->scale_exp[b] = scale_exp_for(dev * 1.0000001f) + 2;  // observed max -> 2^23 range
+    st->l2sq[b] = 0ull;  // recounted by the re-run
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) st->flags = 2;
 }
 
 // Sum the CTAs' partial matrices in a fixed order: block = 32 entries, each of
@@ -414,22 +515,25 @@ __global__ void __launch_bounds__(256) stats_reduce_kernel(const double* __restr
   }
 }
 
-// S = (F + F^T)/2 -> shifted sums (S1, S2, N) -> raw moments in FP64
+// S = (F + F^T)/2, unscaled -> shifted sums (S1, S2, N) -> raw moments in FP64
 // (moments_from_shifted, src/linalg.cpp:81-103).  fsum is column-major:
 // fsum[col * 128 + row] = F[row][col].  Output: sum[B], outer[B*B] (full,
 // symmetric), count.
 __global__ void __launch_bounds__(256) stats_finalize_kernel(const double* __restrict__ fsum,
-                                                            const float* __restrict__ shift, int bands,
+                                                            const StatsState* __restrict__ st, int bands,
                                                             double* __restrict__ moments) {
   __shared__ double s1[kRows];
   __shared__ double r[kRows];
+  __shared__ int ex[kRows];
   const int B = bands;
   auto F = [&](int row, int col) { return fsum[static_cast<size_t>(col) * kRows + row]; };
-  const double N = F(B, B);
+  const double N = ldexp(F(B, B), -2 * kOnesExp);
   for (int i = threadIdx.x; i < B; i += blockDim.x) {
-    s1[i] = 0.5 * (F(i, B) + F(B, i));
-    r[i] = static_cast<double>(shift[i]);
+    ex[i] = st->scale_exp[i];
+    r[i] = static_cast<double>(st->shift[i]);
   }
+  __syncthreads();
+  for (int i = threadIdx.x; i < B; i += blockDim.x) s1[i] = ldexp(0.5 * (F(i, B) + F(B, i)), -(ex[i] + kOnesExp));
   __syncthreads();
   double* sum = moments;
   double* outer = moments + B;
@@ -438,7 +542,9 @@ __global__ void __launch_bounds__(256) stats_finalize_kernel(const double* __res
   for (int e = threadIdx.x; e < B * B; e += blockDim.x) {
     const int i = e / B, j = e % B;
     if (j > i) continue;
-    const double s2 = 0.5 * (F(i, j) + F(j, i));
+    double q = 0.5 * (F(i, j) + F(j, i));
+    if (i == j) q += static_cast<double>(st->l2sq[i]);  // the weight-1 diagonal, exact
+    const double s2 = ldexp(q, -(ex[i] + ex[j]));
     const double v = s2 + r[i] * s1[j] + s1[i] * r[j] + N * r[i] * r[j];
     outer[e] = v;
     outer[j * B + i] = v;
@@ -449,17 +555,19 @@ __global__ void __launch_bounds__(256) stats_finalize_kernel(const double* __res
 // ---------------------------------------------------------------------------
 // Plain FP32 SIMT moments: the comparator path, and the path for B >= 128.
 // Each block owns a 64-band x 64-band tile of the lower triangle over a slice
-// of pixels, 4x4 register blocks per thread, FP32 sums over 1024-pixel chunks
-// flushed into FP64 registers, written to per-block partials, then reduced in
-// a fixed order.  The shift (and ones row) work as in the tensor path.
+// of pixels, 4x4 register blocks per thread, FP32 sums over each 32-pixel
+// staging step flushed into FP64 registers (longer FP32 chains measurably bias
+// the covariance), written to per-block partials, then reduced in a fixed
+// order.  The shift (and ones row) work as in the tensor path.
 // ---------------------------------------------------------------------------
 constexpr int kSimtTile = 64;
 constexpr int kSimtPx = 32;
 
 template <typename T>
 __global__ void __launch_bounds__(256) stats_simt_kernel(const T* __restrict__ cube, int64_t pixels, int64_t stride,
-                                                        int bands, const float* __restrict__ shift,
+                                                        int bands, const StatsState* __restrict__ st,
                                                         double* __restrict__ partials, int slices) {
+  const float* shift = st->shift;
   // blockIdx.x: pixel slice; blockIdx.y: lower-triangle tile pair
   const int tiles = (bands + 1 + kSimtTile - 1) / kSimtTile;  // rows incl. the ones row
   int ti = 0, pair = blockIdx.y;
@@ -512,7 +620,7 @@ __global__ void __launch_bounds__(256) stats_simt_kernel(const T* __restrict__ c
     }
     __syncthreads();
     since_flush += kSimtPx;
-    if (since_flush >= 1024) {
+    if (since_flush >= kSimtPx) {
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
@@ -553,8 +661,9 @@ __global__ void __launch_bounds__(256) simt_reduce_kernel(const double* __restri
 }
 
 __global__ void __launch_bounds__(256) simt_finalize_kernel(const double* __restrict__ fsum, int n,
-                                                           const float* __restrict__ shift, int bands,
+                                                           const StatsState* __restrict__ st, int bands,
                                                            double* __restrict__ moments) {
+  const float* shift = st->shift;
   __shared__ double s1[HSI_MAX_BANDS];
   __shared__ double r[HSI_MAX_BANDS];
   const int B = bands;
@@ -596,33 +705,27 @@ constexpr int kSimtSlices = 96;
 size_t align256(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
 
 struct StatsWorkspace {
-  float* shift;
+  StatsState* state;
   double* partials;
   double* fsum;
 };
 
-size_t ws_bytes(int bands) {
-  const size_t shift = align256(HSI_MAX_BANDS * sizeof(float));
-  if (bands <= kMaxTensorBands) {
-    return shift + align256(static_cast<size_t>(kMaxCtas) * kRows * kRows * sizeof(double)) +
-           align256(kRows * kRows * sizeof(double));
-  }
-  const int n = ((bands + 1 + kSimtTile - 1) / kSimtTile) * kSimtTile;
-  return shift + align256(static_cast<size_t>(kSimtSlices) * n * n * sizeof(double)) +
-         align256(static_cast<size_t>(n) * n * sizeof(double));
+size_t tensor_ws_bytes() {
+  return align256(sizeof(StatsState)) + align256(static_cast<size_t>(kMaxCtas) * kRows * kRows * sizeof(double)) +
+         align256(kRows * kRows * sizeof(double));
 }
 
 size_t simt_ws_bytes(int bands) {
   const int n = ((bands + 1 + kSimtTile - 1) / kSimtTile) * kSimtTile;
-  return align256(HSI_MAX_BANDS * sizeof(float)) + align256(static_cast<size_t>(kSimtSlices) * n * n * sizeof(double)) +
+  return align256(sizeof(StatsState)) + align256(static_cast<size_t>(kSimtSlices) * n * n * sizeof(double)) +
          align256(static_cast<size_t>(n) * n * sizeof(double));
 }
 
 StatsWorkspace carve(void* base, size_t partial_bytes) {
   unsigned char* p = static_cast<unsigned char*>(base);
   StatsWorkspace w;
-  w.shift = reinterpret_cast<float*>(p);
-  p += align256(HSI_MAX_BANDS * sizeof(float));
+  w.state = reinterpret_cast<StatsState*>(p);
+  p += align256(sizeof(StatsState));
   w.partials = reinterpret_cast<double*>(p);
   p += align256(partial_bytes);
   w.fsum = reinterpret_cast<double*>(p);
@@ -645,14 +748,15 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
+// shift + scale -> GEMM -> (conditional) rescale + GEMM re-run -> reduce -> finalize
 template <typename T>
 int launch_tensor_stats(const void* cube, int64_t P, int B, int64_t stride, double* moments, const float* reference,
                         void* workspace, cudaStream_t s, int* status) {
   CUtensorMap map;
-  const int rc = encode_cube_map(&map, cube, sizeof(T) == 4 ? HSI_F32 : HSI_F16, P, B, stride, kKB, kRows);
+  const int rc = encode_cube_map(&map, cube, sizeof(T) == 4 ? HSI_F32 : HSI_F16, P, B, stride, kBoxPx, kRows);
   if (rc != HSI_OK) return rc;
   const StatsWorkspace w = carve(workspace, static_cast<size_t>(kMaxCtas) * kRows * kRows * sizeof(double));
-  shift_kernel<T><<<kRows, 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, reference, w.shift);
+  shift_kernel<T><<<kRows, 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, reference, w.state);
   const int64_t nkb = div_up<int64_t>(P, kKB);
   int grid = num_sms();
   if (grid > kMaxCtas) grid = kMaxCtas;
@@ -668,12 +772,16 @@ int launch_tensor_stats(const void* cube, int64_t P, int B, int64_t stride, doub
   StatsArgs a;
   a.pixels = P;
   a.bands = B;
-  a.shift = w.shift;
+  a.state = w.state;
   a.partials = w.partials;
+  a.conditional = 0;
   a.status = status;
   stats_gemm_kernel<T><<<grid, kThreads, L.total, s>>>(map, a);
+  rescale_kernel<<<1, 128, 0, s>>>(B, w.state);
+  a.conditional = 1;
+  stats_gemm_kernel<T><<<grid, kThreads, L.total, s>>>(map, a);
   stats_reduce_kernel<<<kRows * kRows / 32, 256, 0, s>>>(w.partials, grid, w.fsum);
-  stats_finalize_kernel<<<1, 256, 0, s>>>(w.fsum, w.shift, B, moments);
+  stats_finalize_kernel<<<1, 256, 0, s>>>(w.fsum, w.state, B, moments);
   return static_cast<int>(cudaGetLastError());
 }
 
@@ -683,12 +791,12 @@ int launch_simt_stats(const void* cube, int64_t P, int B, int64_t stride, double
   const int tiles = (B + 1 + kSimtTile - 1) / kSimtTile;
   const int n = tiles * kSimtTile;
   const StatsWorkspace w = carve(workspace, static_cast<size_t>(kSimtSlices) * n * n * sizeof(double));
-  shift_kernel<T><<<HSI_MAX_BANDS, 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, reference, w.shift);
+  shift_kernel<T><<<HSI_MAX_BANDS + 1, 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, reference, w.state);
   const dim3 grid(kSimtSlices, tiles * (tiles + 1) / 2);
-  stats_simt_kernel<T><<<grid, 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, w.shift, w.partials,
+  stats_simt_kernel<T><<<grid, 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, w.state, w.partials,
                                            kSimtSlices);
   simt_reduce_kernel<<<(n * n + 255) / 256, 256, 0, s>>>(w.partials, kSimtSlices, n, w.fsum);
-  simt_finalize_kernel<<<1, 256, 0, s>>>(w.fsum, n, w.shift, B, moments);
+  simt_finalize_kernel<<<1, 256, 0, s>>>(w.fsum, n, w.state, B, moments);
   return static_cast<int>(cudaGetLastError());
 }
 
@@ -725,7 +833,7 @@ using namespace hsi_b200;
 
 extern "C" HSI_API size_t hsi_stats_workspace_bytes(int height, int width, int bands) {
   if (height <= 0 || width <= 0 || bands <= 0 || bands > HSI_MAX_BANDS) return 0;
-  const size_t a = ws_bytes(bands), b = simt_ws_bytes(bands);
+  const size_t a = tensor_ws_bytes(), b = simt_ws_bytes(bands);
   return a > b ? a : b;
 }
 
@@ -737,7 +845,10 @@ extern "C" HSI_API int hsi_scene_moments(const void* d_cube, int height, int wid
   if (!d_workspace || workspace_bytes < hsi_stats_workspace_bytes(height, width, bands)) return HSI_E_WORKSPACE;
   const int64_t P = static_cast<int64_t>(height) * width;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (bands <= kMaxTensorBands) {
+  // The integer path's one approximation (the off-diagonal sums of the
+  // lowest limbs' products) shrinks as 1/sqrt(pixels); small frames, which
+  // are also cheap, take the FP32 CUDA-core path.
+  if (bands <= kMaxTensorBands && P >= kTensorMinPixels) {
     return dtype == HSI_F32 ? launch_tensor_stats<float>(d_cube, P, bands, plane_stride, d_moments, d_reference,
                                                          d_workspace, s, nullptr)
                             : launch_tensor_stats<__half>(d_cube, P, bands, plane_stride, d_moments, d_reference,
@@ -759,4 +870,19 @@ extern "C" HSI_API int hsi_scene_moments_simt(const void* d_cube, int height, in
   return dtype == HSI_F32
              ? launch_simt_stats<float>(d_cube, P, bands, plane_stride, d_moments, d_reference, d_workspace, s)
              : launch_simt_stats<__half>(d_cube, P, bands, plane_stride, d_moments, d_reference, d_workspace, s);
+}
+
+extern "C" HSI_API int hsi_scene_moments_tc(const void* d_cube, int height, int width, int bands, int dtype,
+                                            int64_t plane_stride, double* d_moments, const float* d_reference,
+                                            void* d_workspace, size_t workspace_bytes, hsi_stream_t stream) {
+  const int rc = check_common(d_cube, height, width, bands, dtype, plane_stride, d_moments);
+  if (rc != HSI_OK) return rc;
+  if (bands > kMaxTensorBands) return HSI_E_CAPACITY;
+  if (!d_workspace || workspace_bytes < hsi_stats_workspace_bytes(height, width, bands)) return HSI_E_WORKSPACE;
+  const int64_t P = static_cast<int64_t>(height) * width;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return dtype == HSI_F32 ? launch_tensor_stats<float>(d_cube, P, bands, plane_stride, d_moments, d_reference,
+                                                       d_workspace, s, nullptr)
+                          : launch_tensor_stats<__half>(d_cube, P, bands, plane_stride, d_moments, d_reference,
+                                                        d_workspace, s, nullptr);
 }

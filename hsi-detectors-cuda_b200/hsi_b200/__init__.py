@@ -114,11 +114,14 @@ def _optional_symbols(L):
         "hsi_stats_workspace_bytes": ([i32, i32, i32], C.c_size_t),
         "hsi_scene_moments": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
         "hsi_scene_moments_simt": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
+        "hsi_scene_moments_tc": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
         "hsi_statistics_elements": ([i32, i32], C.c_size_t),
         "hsi_factor_workspace_bytes": ([i32, i32], C.c_size_t),
         "hsi_build_statistics": ([i32, i32, i32, f64, vp, vp, i64, vp, vp, vp, vp, vp, C.c_size_t, vp], i32),
-        "hsi_rx_ace": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, vp, i32, vp, vp, vp, vp, i64, vp], i32),
-        "hsi_rx_ace_simt": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, vp, i32, vp, vp, vp, vp, i64, vp], i32),
+        "hsi_rx_ace_workspace_bytes": ([i32, i32], C.c_size_t),
+        "hsi_rx_ace": ([vp, i32, i32, i32, i32, i64, vp, i32, vp, vp, vp, vp, i64, vp, C.c_size_t, vp], i32),
+        "hsi_rx_ace_simt_workspace_bytes": ([i32, i32], C.c_size_t),
+        "hsi_rx_ace_simt": ([vp, i32, i32, i32, i32, i64, vp, i32, vp, vp, vp, vp, i64, vp, C.c_size_t, vp], i32),
         "hsi_demosaic": ([vp, i32, i32, i32, i32, vp, vp, i64, vp], i32),
     }
     for name, (argtypes, restype) in table.items():
@@ -305,9 +308,10 @@ def moments_elements(bands) -> int:
 
 
 def scene_moments(cube, height, width, bands, dtype=F32, stride=None, out=None, reference=None, workspace=None,
-                  simt=False, stream=None):
+                  simt=False, path=None, stream=None):
     """Raw moments of one frame on the device: (B + B*B + 1,) float64 = sum, outer, count
-    (the reference's SpectralMoments).  simt=True uses the plain FP32 CUDA-core path."""
+    (the reference's SpectralMoments).  path: None (automatic), "simt" (plain FP32
+    CUDA cores) or "tc" (integer tensor cores at any size)."""
     torch = _torch()
     dev = cube.device
     stride = cube.shape[-1] if stride is None else stride
@@ -315,7 +319,9 @@ def scene_moments(cube, height, width, bands, dtype=F32, stride=None, out=None, 
         out = torch.empty(moments_elements(bands), dtype=torch.float64, device=dev)
     if workspace is None:
         workspace = torch.empty(stats_workspace_bytes(height, width, bands), dtype=torch.uint8, device=dev)
-    fn = lib().hsi_scene_moments_simt if simt else lib().hsi_scene_moments
+    path = "simt" if simt else path
+    fn = {None: lib().hsi_scene_moments, "simt": lib().hsi_scene_moments_simt,
+          "tc": lib().hsi_scene_moments_tc}[path]
     check(fn(_ptr(cube), height, width, bands, dtype, stride, _ptr(out), _ptr(reference), _ptr(workspace),
              workspace.numel(), _stream(stream)), "hsi_scene_moments")
     return out
@@ -367,3 +373,27 @@ def build_statistics(moments, bands, library=None, loading=1e-6, want64=True, wa
                                      _ptr(s64), _ptr(s32), _ptr(cem_weights), _ptr(status), _ptr(ws), wsb,
                                      _stream(stream)), "hsi_build_statistics")
     return s64, s32, status
+
+
+# ---------------------------------------------------------------------------
+# RX / ACE scoring
+# ---------------------------------------------------------------------------
+
+def rx_ace(cube, height, width, bands, stats64, num_targets, dtype=F32, stride=None, rx=None, ace_best=None,
+           ace_target=None, ace_maps=None, map_stride=None, simt=False, workspace=None, stream=None):
+    """RX and ACE maps of one frame from its packed FP64 statistics (build_statistics).
+    simt=True runs the plain FP32 CUDA-core path."""
+    torch = _torch()
+    dev = cube.device
+    stride = cube.shape[-1] if stride is None else stride
+    P = height * width
+    L = lib()
+    wsf = L.hsi_rx_ace_simt_workspace_bytes if simt else L.hsi_rx_ace_workspace_bytes
+    fn = L.hsi_rx_ace_simt if simt else L.hsi_rx_ace
+    if workspace is None:
+        workspace = torch.empty(wsf(bands, num_targets), dtype=torch.uint8, device=dev)
+    if map_stride is None:
+        map_stride = ace_maps.shape[-1] if ace_maps is not None else P
+    check(fn(_ptr(cube), height, width, bands, dtype, stride, _ptr(stats64), num_targets, _ptr(rx), _ptr(ace_best),
+             _ptr(ace_target), _ptr(ace_maps), map_stride, _ptr(workspace), workspace.numel(), _stream(stream)),
+          "hsi_rx_ace")

@@ -174,27 +174,33 @@ HSI_API int hsi_score_frames_device(const hsi_frame* d_frames, int num_frames, i
                                     int max_sam, int max_cem, int* d_status, hsi_stream_t stream);
 
 /* ---- scene statistics -------------------------------------------------------
- * Raw first and second moments of one frame, on the tensor cores: sums about a
- * per-band reference r (near the mean) split into BF16 hi/lo parts, FP32
- * accumulation in TMEM over 1024-pixel chunks folded into FP64, then rebuilt
- * as raw moments in FP64.  Output `d_moments` (FP64): sum[B], outer[B*B]
- * (full symmetric), count -- the contents of hsi::SpectralMoments.  Replaces
- * the reference's launch_reset_moments / launch_accumulate_mean /
- * launch_accumulate_moments / read_moments (include/hsi/stats_cuda.hpp:26-72,
- * src/stats.cu:169-248) and accumulate_moments_cpu
- * (src/detectors_cpu.cpp:77-93).  `d_reference` (nullable, `bands` floats):
- * the shift, e.g. the previous frame's mean; null samples the frame.
- * Tensor-core path for bands <= 127; 128..256 bands use the FP32 SIMT path.
+ * Raw first and second moments of one frame.  Output `d_moments` (FP64):
+ * sum[B], outer[B*B] (full symmetric), count -- the contents of
+ * hsi::SpectralMoments.  Replaces the reference's launch_reset_moments /
+ * launch_accumulate_mean / launch_accumulate_moments / read_moments
+ * (include/hsi/stats_cuda.hpp:26-72, src/stats.cu:169-248) and
+ * accumulate_moments_cpu (src/detectors_cpu.cpp:77-93).
+ * Sums are taken about a per-band reference r near the mean (`d_reference`,
+ * `bands` floats, e.g. the previous frame's mean; null: a subsample mean) and
+ * rebuilt as raw moments in FP64.
+ * Tensor-core path (bands <= 127, >= 32768 pixels): fixed-point (x - r) split
+ * into signed 8-bit limbs, exact INT32 accumulation on tcgen05 (kind::i8),
+ * FP64 reduction.  Otherwise the FP32 CUDA-core path below.
  */
 HSI_API size_t hsi_stats_workspace_bytes(int height, int width, int bands);
 HSI_API int hsi_scene_moments(const void* d_cube, int height, int width, int bands, int dtype,
                               int64_t plane_stride, double* d_moments, const float* d_reference,
                               void* d_workspace, size_t workspace_bytes, hsi_stream_t stream);
 /* Same moments with plain FP32 CUDA-core arithmetic (register-blocked, FP32
- * chunks folded into FP64): the comparator for the tensor-core path. */
+ * sums over 32-pixel steps folded into FP64): the comparator for the
+ * tensor-core path, and the path for small frames and bands >= 128. */
 HSI_API int hsi_scene_moments_simt(const void* d_cube, int height, int width, int bands, int dtype,
                                    int64_t plane_stride, double* d_moments, const float* d_reference,
                                    void* d_workspace, size_t workspace_bytes, hsi_stream_t stream);
+/* The tensor-core path at any frame size (bands <= 127, else HSI_E_CAPACITY). */
+HSI_API int hsi_scene_moments_tc(const void* d_cube, int height, int width, int bands, int dtype,
+                                 int64_t plane_stride, double* d_moments, const float* d_reference,
+                                 void* d_workspace, size_t workspace_bytes, hsi_stream_t stream);
 
 /* ---- detector statistics (FP64 factorisation) --------------------------------
  * For each of `num_frames` frames (moments contiguous, B + B*B + 1 doubles
@@ -219,6 +225,24 @@ HSI_API int hsi_build_statistics(int num_frames, int bands, int num_targets, dou
                                  const double* d_moments, const float* d_library, int64_t library_stride,
                                  double* d_stats64, float* d_stats32, float* d_cem_weights, int* d_status,
                                  void* d_workspace, size_t workspace_bytes, hsi_stream_t stream);
+
+/* ---- RX / ACE scoring ----------------------------------------------------------
+ * RX = |W (x - mu)|^2 and ACE_t = (z . u_t)^2 / (|u_t|^2 |z|^2) for every
+ * pixel, from the frame's packed FP64 statistics (hsi_build_statistics),
+ * with the reference's rules: a target is skipped (ACE 0) when |u_t|^2 <= 0 or
+ * |z|^2 <= 0; the best is the largest ACE, lowest t on ties, clamped to [0, 1];
+ * score 0 and target -1 when no target is valid (reference rx_cpu /
+ * ace_best_cpu, src/detectors_cpu.cpp:95-156; the reference has no GPU RX/ACE).
+ * Outputs are each nullable: `d_rx` (P floats), `d_ace_best` (P), `d_ace_target`
+ * (P int32), `d_ace_maps` (num_targets maps at `map_stride`).  At most 16
+ * targets per call.
+ */
+HSI_API size_t hsi_rx_ace_simt_workspace_bytes(int bands, int num_targets);
+/* Plain FP32 CUDA-core path (register-blocked GEMM over [W; (W^T U)^T]). */
+HSI_API int hsi_rx_ace_simt(const void* d_cube, int height, int width, int bands, int dtype,
+                            int64_t plane_stride, const double* d_stats64, int num_targets, float* d_rx,
+                            float* d_ace_best, int32_t* d_ace_target, float* d_ace_maps, int64_t map_stride,
+                            void* d_workspace, size_t workspace_bytes, hsi_stream_t stream);
 
 /* ---- detection compaction ---------------------------------------------------
  * Threshold + non-maximum suppression + compaction of one score map into a

@@ -3,7 +3,8 @@ factorisation against the FP64 oracle and the reference's own fixtures.
 
 Tolerances (stated here):
   moments      : count exact; mean relative error < 1e-7; covariance entries
-                 within 1e-6 of the largest covariance entry;
+                 within 5e-8 of the largest covariance entry (RX/ACE amplify
+                 covariance errors by the condition number, ~4000 here);
   statistics   : from the same FP64 moments, every FP64 statistic within
                  1e-9 relative (different order of FP64 operations);
   RX           : |gpu - fp64| / max(1, |fp64|) <= 1e-4  (the reference's
@@ -26,7 +27,7 @@ def _cov(s, o, n):
     return o / n - np.outer(mu, mu), mu
 
 
-def _check_moments(hsi, orc, host, gm, B, P):
+def _check_moments(hsi, orc, host, gm, B, P, cov_tol=5e-8):
     s0, o0, n0 = orc.moments(host)
     s, o, n = [x.cpu().numpy() for x in hsi.split_moments(gm, B)]
     assert float(n) == P == n0
@@ -35,22 +36,26 @@ def _check_moments(hsi, orc, host, gm, B, P):
     assert np.max(np.abs(mu - mu0) / np.maximum(np.abs(mu0), 1e-3)) < 1e-7
     scale = np.max(np.abs(c0))
     err = np.max(np.abs(c - c0)) / max(scale, 1e-30)
-    assert err < 1e-6, f"covariance error {err:.3e} of max entry"
+    assert err < cov_tol, f"covariance error {err:.3e} of max entry"
     assert np.allclose(o, o.T, rtol=0, atol=0)
     return err
 
 
-@pytest.mark.parametrize("simt", [False, True])
+@pytest.mark.parametrize("path", [None, "simt", "tc"])
 @pytest.mark.parametrize("B", [1, 3, 16, 113, 127, 128, 224])
 @pytest.mark.parametrize("shape", [(7, 13), (64, 64), (256, 300)])
-def test_moments_match_fp64(hsi, orc, simt, B, shape):
+def test_moments_match_fp64(hsi, orc, path, B, shape):
     H, W = shape
+    if path == "tc" and B > 127:
+        pytest.skip("tensor-core path holds at most 127 bands")
     sc = hsi.scene(B, n_targets=2, target_frac=0.01, anomaly_frac=0.005, frame_seed=B * 31 + H)
     cube, _ = hsi.generate(sc, H, W)
     host = _download(cube, B, H * W)
-    gm = hsi.scene_moments(cube, H, W, B, simt=simt)
+    gm = hsi.scene_moments(cube, H, W, B, path=path)
     torch.cuda.synchronize()
-    _check_moments(hsi, orc, host, gm, B, H * W)
+    # the forced integer path on tiny frames: its zero-mean residue shrinks as 1/sqrt(N)
+    tol = max(5e-8, 1e-6 / np.sqrt(H * W / 100.0)) if path == "tc" else 5e-8
+    _check_moments(hsi, orc, host, gm, B, H * W, cov_tol=tol)
 
 
 @pytest.mark.parametrize("dtype", [0, 1])
