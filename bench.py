@@ -249,6 +249,11 @@ class Workload:
         self.counts = torch.zeros((frames,), dtype=torch.int32, device=device)
         self.ws_bytes = hsi.detect_workspace_bytes(H, W)
         self.ws = torch.empty((frames, self.ws_bytes), dtype=torch.uint8, device=device)
+        # one batched detection call for every frame's best-angle map
+        self.jobs = [hsi.detect_job(self.sam_best[f], self.sam_bt[f], H, W, THRESHOLD, NMS_RADIUS,
+                                    hsi.LOWER_IS_BETTER, CAPACITY, self.dets[f], self.counts[f:f + 1])
+                     for f in range(frames)]
+        self.det_ws = torch.empty(hsi.detect_batch_workspace_bytes(self.jobs), dtype=torch.uint8, device=device)
         self.cem = self.kind == "sam_cem"
         if self.cem:
             self.cem_w = torch.zeros((frames, TARGETS, B), device=device)
@@ -303,10 +308,8 @@ class Workload:
         if events is not None:
             events[1].record(stream)
         self.counts.zero_()
-        for f in range(self.n):
-            hsi.detect(self.sam_best[f], self.sam_bt[f], H, W, THRESHOLD, NMS_RADIUS, hsi.LOWER_IS_BETTER,
-                       CAPACITY, out=self.dets[f], count=self.counts[f:f + 1], workspace=self.ws[f], stream=stream)
-            launches += 3
+        hsi.detect_batch(self.jobs, self.det_ws, stream=stream)
+        launches += 3
         return launches
 
     # shift, GEMM, conditional rescale + re-run, reduce, finalize

@@ -9,7 +9,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/hsi_b200.h"
+#include "hsi_b200.h"
 
 namespace hsi_b200 {
 

@@ -1,13 +1,17 @@
 // detect.cu - threshold + non-maximum suppression + ordered compaction.
 //
-// Three small launches, no atomics on the data path, so the list comes out in
-// raster order and is identical run to run:
-//   1. flags:  per 2048-pixel tile, every pixel's pass/fail as a warp ballot
-//              word (bitmask in the workspace) and the tile's count;
-//   2. scan:   one block turns the tile counts into output offsets, starting
-//              at the caller's *d_count, and advances *d_count by the total;
-//   3. emit:   each tile writes its detections at its offset + in-tile rank,
-//              dropping (but having counted) those past capacity.
+// Three launches for a whole batch of score maps, no atomics on the data
+// path, so every list comes out in raster order and is identical run to run:
+//   1. flags:  per row segment (up to 2048 pixels of one row), every pixel's
+//              pass/fail as warp ballot words (bitmask in the workspace) and
+//              the segment's count.  The score rows the NMS window needs are
+//              staged in shared memory (radius <= 4; larger radii read global
+//              memory), padded with NaN so out-of-frame neighbours never win
+//              or tie, exactly like the bounds checks of the CPU loop;
+//   2. scan:   one block per map turns segment counts into output offsets,
+//              starting at the caller's *count, and advances *count;
+//   3. emit:   each segment writes its detections at offset + in-segment
+//              rank, dropping (but having counted) those past capacity.
 // Semantics are the reference CPU path's (src/sam_cpu.cpp:86-138), polarity
 // included; the reference GPU kernel (src/detect.cu:43-87) ignores polarity
 // and emits in atomic arrival order, both of which this replaces.
@@ -18,32 +22,48 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kPerThread = 8;
-constexpr int kTilePixels = kThreads * kPerThread;  // 2048
-constexpr int kWordsPerTile = kTilePixels / 32;      // 64
+constexpr int kSeg = kThreads * kPerThread;  // 2048 pixels per segment
+constexpr int kWordsPerSeg = kSeg / 32;      // 64
+constexpr int kMaxStagedRadius = 4;
+constexpr int kMaxJobs = 64;
 
-struct DetectWorkspace {
-  uint32_t* counts;   // [tiles]
-  uint32_t* offsets;  // [tiles]
-  uint32_t* masks;    // [tiles * 64]
+struct Job {
+  const float* score;
+  const int32_t* target;
+  int height, width;
+  float threshold;
+  int radius;
+  int higher;
+  int capacity;
+  hsi_detection* out;
+  uint32_t* count;
+  int seg0;          // first segment of this map in the batch
+  int segs_per_row;  // ceil(width / kSeg)
 };
 
-size_t tiles_for(int64_t pixels) { return static_cast<size_t>(div_up<int64_t>(pixels, kTilePixels)); }
+struct Batch {
+  Job jobs[kMaxJobs];
+  int njobs;
+  int total_segs;
+  uint32_t* counts;   // [total_segs]
+  uint32_t* offsets;  // [total_segs]
+  uint32_t* masks;    // [total_segs * 64]
+};
 
-size_t workspace_bytes(int64_t pixels) {
-  const size_t t = tiles_for(pixels);
-  return t * sizeof(uint32_t) * (2 + kWordsPerTile) + 256;
-}
-
-DetectWorkspace carve(void* base, int64_t pixels) {
-  const size_t t = tiles_for(pixels);
-  uint32_t* p = static_cast<uint32_t*>(base);
-  return DetectWorkspace{p, p + t, p + 2 * t};
+__device__ __forceinline__ int find_job(const Batch& b, int seg) {
+  int lo = 0, hi = b.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (b.jobs[mid].seg0 <= seg) lo = mid; else hi = mid - 1;
+  }
+  return lo;
 }
 
 __device__ __forceinline__ bool better(float a, float b, bool higher) { return higher ? a > b : a < b; }
 
-__device__ bool local_best(const float* __restrict__ s, int x, int y, int w, int h, int r, float self,
-                           bool higher) {
+// NMS against global memory, for radii too large to stage.
+__device__ bool local_best_global(const float* __restrict__ s, int x, int y, int w, int h, int r, float self,
+                                  bool higher) {
   const int64_t self_idx = static_cast<int64_t>(y) * w + x;
   for (int dy = -r; dy <= r; ++dy) {
     const int ny = y + dy;
@@ -61,51 +81,92 @@ __device__ bool local_best(const float* __restrict__ s, int x, int y, int w, int
   return true;
 }
 
-__global__ void __launch_bounds__(kThreads) detect_flags_kernel(const float* __restrict__ score, int width,
-                                                                int height, float threshold, int radius,
-                                                                bool higher, DetectWorkspace ws) {
-  const int64_t pixels = static_cast<int64_t>(width) * height;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(kThreads) flags_kernel(const __grid_constant__ Batch b) {
+  extern __shared__ float tile[];  // (2r+1) rows x (kSeg + 2r) columns
   __shared__ uint32_t s_count[kThreads / 32];
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * kTilePixels;
-  uint32_t mine = 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int seg = blockIdx.x; seg < b.total_segs; seg += gridDim.x) {
+    __syncthreads();  // the previous segment is done with the tile and s_count
+    const Job& J = b.jobs[find_job(b, seg)];
+    const int local = seg - J.seg0;
+    const int y = local / J.segs_per_row;
+    const int x0 = (local % J.segs_per_row) * kSeg;
+    const int len = min(kSeg, J.width - x0);
+    const int r = J.radius > 0 ? J.radius : 0;
+    const bool staged = r <= kMaxStagedRadius;
+    const bool higher = J.higher != 0;
+    const int tw = kSeg + 2 * r;
+    if (r > 0 && staged) {
+      const int rows = 2 * r + 1;
+      for (int e = threadIdx.x; e < rows * (len + 2 * r); e += kThreads) {
+        const int ry = e / (len + 2 * r), rx = e % (len + 2 * r);
+        const int gy = y - r + ry, gx = x0 - r + rx;
+        float v = __int_as_float(0x7fc00000);  // NaN: never better, never equal
+        if (gy >= 0 && gy < J.height && gx >= 0 && gx < J.width)
+          v = J.score[static_cast<int64_t>(gy) * J.width + gx];
+        tile[ry * tw + rx] = v;
+      }
+      __syncthreads();
+    }
+    uint32_t mine = 0;
 #pragma unroll
-  for (int i = 0; i < kPerThread; ++i) {
-    const int64_t p = base + i * kThreads + threadIdx.x;
-    bool pass = false;
-    if (p < pixels) {
-      const float s = score[p];
-      const bool over = higher ? (s >= threshold) : (s <= threshold);
-      if (over) {
-        const int x = static_cast<int>(p % width), y = static_cast<int>(p / width);
-        pass = radius <= 0 || local_best(score, x, y, width, height, radius, s, higher);
+    for (int i = 0; i < kPerThread; ++i) {
+      const int xi = i * kThreads + threadIdx.x;  // pixel within the segment
+      bool pass = false;
+      if (xi < len) {
+        const int x = x0 + xi;
+        const float s = J.score[static_cast<int64_t>(y) * J.width + x];
+        const bool over = higher ? (s >= J.threshold) : (s <= J.threshold);
+        if (over) {
+          if (r == 0) {
+            pass = true;
+          } else if (staged) {
+            pass = true;
+            const float* c = tile + r * tw + (xi + r);  // centre of the window
+            for (int dy = -r; dy <= r && pass; ++dy) {
+              for (int dx = -r; dx <= r; ++dx) {
+                if (dx == 0 && dy == 0) continue;
+                const float o = c[dy * tw + dx];
+                if (better(o, s, higher) || (o == s && (dy < 0 || (dy == 0 && dx < 0)))) {
+                  pass = false;
+                  break;
+                }
+              }
+            }
+          } else {
+            pass = local_best_global(J.score, x, y, J.width, J.height, r, s, higher);
+          }
+        }
+      }
+      const uint32_t word = __ballot_sync(0xffffffffu, pass);
+      if (lane == 0) {
+        b.masks[static_cast<int64_t>(seg) * kWordsPerSeg + i * (kThreads / 32) + warp] = word;
+        mine += __popc(word);
       }
     }
-    const uint32_t word = __ballot_sync(0xffffffffu, pass);
-    if (lane == 0) {
-      ws.masks[static_cast<int64_t>(blockIdx.x) * kWordsPerTile + i * (kThreads / 32) + warp] = word;
-      mine += __popc(word);
+    if (lane == 0) s_count[warp] = mine;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t total = 0;
+      for (int w = 0; w < kThreads / 32; ++w) total += s_count[w];
+      b.counts[seg] = total;
     }
-  }
-  if (lane == 0) s_count[warp] = mine;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t total = 0;
-    for (int w = 0; w < kThreads / 32; ++w) total += s_count[w];
-    ws.counts[blockIdx.x] = total;
   }
 }
 
-// Single block: exclusive scan of tile counts starting at *count; *count += total.
-__global__ void __launch_bounds__(1024) detect_scan_kernel(int tiles, DetectWorkspace ws, uint32_t* count) {
+// One block per map: exclusive scan of its segment counts from *count;
+// *count += total.
+__global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ Batch b) {
   __shared__ uint32_t s_warp[32];
   __shared__ uint32_t s_carry;
+  const Job& J = b.jobs[blockIdx.x];
+  const int segs = J.height * J.segs_per_row;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) s_carry = *count;
+  if (threadIdx.x == 0) s_carry = *J.count;
   __syncthreads();
-  for (int chunk = 0; chunk < tiles; chunk += 1024) {
+  for (int chunk = 0; chunk < segs; chunk += 1024) {
     const int i = chunk + threadIdx.x;
-    const uint32_t v = i < tiles ? ws.counts[i] : 0u;
+    const uint32_t v = i < segs ? b.counts[J.seg0 + i] : 0u;
     uint32_t incl = v;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -121,63 +182,132 @@ __global__ void __launch_bounds__(1024) detect_scan_kernel(int tiles, DetectWork
         const uint32_t o = __shfl_up_sync(0xffffffffu, w, d);
         if (lane >= d) w += o;
       }
-      s_warp[lane] = w;  // inclusive over warps
+      s_warp[lane] = w;
     }
     __syncthreads();
     const uint32_t warp_base = warp > 0 ? s_warp[warp - 1] : 0u;
     const uint32_t carry = s_carry;
-    if (i < tiles) ws.offsets[i] = carry + warp_base + incl - v;
+    if (i < segs) b.offsets[J.seg0 + i] = carry + warp_base + incl - v;
     __syncthreads();
     if (threadIdx.x == 0) s_carry = carry + s_warp[31];
     __syncthreads();
   }
-  if (threadIdx.x == 0) *count = s_carry;
+  if (threadIdx.x == 0) *J.count = s_carry;
 }
 
-__global__ void __launch_bounds__(kThreads) detect_emit_kernel(const float* __restrict__ score,
-                                                               const int32_t* __restrict__ target, int width,
-                                                               int capacity, DetectWorkspace ws,
-                                                               hsi_detection* __restrict__ out) {
-  __shared__ uint32_t s_words[kWordsPerTile];
-  __shared__ uint32_t s_prefix[kWordsPerTile];
-  const int64_t tile = blockIdx.x;
-  if (threadIdx.x < kWordsPerTile) s_words[threadIdx.x] = ws.masks[tile * kWordsPerTile + threadIdx.x];
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    // exclusive prefix of popcounts over the 64 words, two per lane
-    const int lane = threadIdx.x;
-    const uint32_t a = __popc(s_words[2 * lane]), b = __popc(s_words[2 * lane + 1]);
-    uint32_t incl = a + b;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
-      if (lane >= d) incl += o;
-    }
-    const uint32_t excl = incl - a - b;
-    s_prefix[2 * lane] = excl;
-    s_prefix[2 * lane + 1] = excl + a;
-  }
-  __syncthreads();
-  const uint32_t base = ws.offsets[tile];
+__global__ void __launch_bounds__(kThreads) emit_kernel(const __grid_constant__ Batch b) {
+  __shared__ uint32_t s_words[kWordsPerSeg];
+  __shared__ uint32_t s_prefix[kWordsPerSeg];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t lt = (1u << lane) - 1u;
+  for (int seg = blockIdx.x; seg < b.total_segs; seg += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x < kWordsPerSeg) s_words[threadIdx.x] = b.masks[static_cast<int64_t>(seg) * kWordsPerSeg + threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const uint32_t a = __popc(s_words[2 * lane]), c = __popc(s_words[2 * lane + 1]);
+      uint32_t incl = a + c;
 #pragma unroll
-  for (int i = 0; i < kPerThread; ++i) {
-    const int w = i * (kThreads / 32) + warp;
-    const uint32_t word = s_words[w];
-    if ((word >> lane) & 1u) {
-      const uint32_t slot = base + s_prefix[w] + __popc(word & lt);
-      if (slot < static_cast<uint32_t>(capacity)) {
-        const int64_t p = tile * kTilePixels + static_cast<int64_t>(w) * 32 + lane;
-        hsi_detection d;
-        d.x = static_cast<int32_t>(p % width);
-        d.y = static_cast<int32_t>(p / width);
-        d.target = target ? target[p] : 0;
-        d.score = score[p];
-        out[slot] = d;
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += o;
+      }
+      const uint32_t excl = incl - a - c;
+      s_prefix[2 * lane] = excl;
+      s_prefix[2 * lane + 1] = excl + a;
+    }
+    __syncthreads();
+    const Job& J = b.jobs[find_job(b, seg)];
+    const int local = seg - J.seg0;
+    const int y = local / J.segs_per_row;
+    const int x0 = (local % J.segs_per_row) * kSeg;
+    const uint32_t base = b.offsets[seg];
+    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int i = 0; i < kPerThread; ++i) {
+      const int w = i * (kThreads / 32) + warp;
+      const uint32_t word = s_words[w];
+      if ((word >> lane) & 1u) {
+        const uint32_t slot = base + s_prefix[w] + __popc(word & lt);
+        if (slot < static_cast<uint32_t>(J.capacity)) {
+          const int x = x0 + w * 32 + lane;
+          const int64_t p = static_cast<int64_t>(y) * J.width + x;
+          hsi_detection d;
+          d.x = x;
+          d.y = y;
+          d.target = J.target ? J.target[p] : 0;
+          d.score = J.score[p];
+          J.out[slot] = d;
+        }
       }
     }
   }
+}
+
+int segs_of(int height, int width) { return height * ((width + kSeg - 1) / kSeg); }
+
+size_t ws_bytes_for_segs(int64_t segs) { return static_cast<size_t>(segs) * sizeof(uint32_t) * (2 + kWordsPerSeg) + 256; }
+
+int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cudaStream_t s) {
+  if (!jobs || n <= 0 || n > kMaxJobs) return HSI_E_INVALID;
+  Batch b{};
+  int64_t segs = 0;
+  int max_r = 0;
+  for (int i = 0; i < n; ++i) {
+    const hsi_detect_job& j = jobs[i];
+    if (!j.score || !j.count || j.height <= 0 || j.width <= 0 || j.capacity < 0) return HSI_E_INVALID;
+    if (j.capacity > 0 && !j.out) return HSI_E_INVALID;
+    if (j.polarity != HSI_LOWER_IS_BETTER && j.polarity != HSI_HIGHER_IS_BETTER) return HSI_E_INVALID;
+    Job& J = b.jobs[i];
+    J.score = j.score;
+    J.target = j.target;
+    J.height = j.height;
+    J.width = j.width;
+    J.threshold = j.threshold;
+    J.radius = j.nms_radius;
+    J.higher = j.polarity == HSI_HIGHER_IS_BETTER;
+    J.capacity = j.capacity;
+    J.out = j.out;
+    J.count = j.count;
+    J.seg0 = static_cast<int>(segs);
+    J.segs_per_row = (j.width + kSeg - 1) / kSeg;
+    segs += segs_of(j.height, j.width);
+    // staged radii size the shared tile; larger ones read global memory
+    if (j.nms_radius <= kMaxStagedRadius && j.nms_radius > max_r) max_r = j.nms_radius;
+  }
+  if (segs > 0x3fffffff) return HSI_E_CAPACITY;
+  if (!ws || ws_bytes < ws_bytes_for_segs(segs)) return HSI_E_WORKSPACE;
+  if ((reinterpret_cast<uintptr_t>(ws) & 15u) != 0) return HSI_E_INVALID;
+  b.njobs = n;
+  b.total_segs = static_cast<int>(segs);
+  uint32_t* p = static_cast<uint32_t*>(ws);
+  b.counts = p;
+  b.offsets = p + segs;
+  b.masks = p + 2 * segs;
+  const size_t smem = static_cast<size_t>(2 * max_r + 1) * (kSeg + 2 * max_r) * sizeof(float);
+  static bool configured = false;
+  if (!configured) {
+    const cudaError_t e = cudaFuncSetAttribute(flags_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>((2 * kMaxStagedRadius + 1) *
+                                                                (kSeg + 2 * kMaxStagedRadius) * sizeof(float)));
+    if (e != cudaSuccess) return static_cast<int>(e);
+    configured = true;
+  }
+  const int grid = static_cast<int>(segs < 16 * sm_count() ? segs : 16 * sm_count());
+  flags_kernel<<<grid, kThreads, smem, s>>>(b);
+  scan_kernel<<<n, 1024, 0, s>>>(b);
+  emit_kernel<<<grid, kThreads, 0, s>>>(b);
+  return static_cast<int>(cudaGetLastError());
 }
 
 }  // namespace
@@ -187,28 +317,38 @@ using namespace hsi_b200;
 
 extern "C" HSI_API size_t hsi_detect_workspace_bytes(int height, int width) {
   if (height <= 0 || width <= 0) return 0;
-  return workspace_bytes(static_cast<int64_t>(height) * width);
+  return ws_bytes_for_segs(segs_of(height, width));
+}
+
+extern "C" HSI_API size_t hsi_detect_batch_workspace_bytes(const hsi_detect_job* jobs, int num_jobs) {
+  if (!jobs || num_jobs <= 0) return 0;
+  int64_t segs = 0;
+  for (int i = 0; i < num_jobs; ++i) {
+    if (jobs[i].height <= 0 || jobs[i].width <= 0) return 0;
+    segs += segs_of(jobs[i].height, jobs[i].width);
+  }
+  return ws_bytes_for_segs(segs);
 }
 
 extern "C" HSI_API int hsi_detect(const float* d_score, const int32_t* d_target, int height, int width,
                                   float threshold, int nms_radius, int polarity, int capacity,
                                   hsi_detection* d_out, uint32_t* d_count, void* d_workspace,
-                                  size_t workspace_bytes_given, hsi_stream_t stream) {
-  if (!d_score || !d_count || height <= 0 || width <= 0 || capacity < 0) return HSI_E_INVALID;
-  if (capacity > 0 && !d_out) return HSI_E_INVALID;
-  if (polarity != HSI_LOWER_IS_BETTER && polarity != HSI_HIGHER_IS_BETTER) return HSI_E_INVALID;
-  const int64_t pixels = static_cast<int64_t>(height) * width;
-  if (!d_workspace || workspace_bytes_given < workspace_bytes(pixels)) return HSI_E_WORKSPACE;
-  if ((reinterpret_cast<uintptr_t>(d_workspace) & 15u) != 0) return HSI_E_INVALID;
-  const size_t tiles = tiles_for(pixels);
-  if (tiles > 0x7fffffff) return HSI_E_CAPACITY;
-  const DetectWorkspace ws = carve(d_workspace, pixels);
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const bool higher = polarity == HSI_HIGHER_IS_BETTER;
-  detect_flags_kernel<<<static_cast<unsigned>(tiles), kThreads, 0, s>>>(d_score, width, height, threshold,
-                                                                      nms_radius, higher, ws);
-  detect_scan_kernel<<<1, 1024, 0, s>>>(static_cast<int>(tiles), ws, d_count);
-  detect_emit_kernel<<<static_cast<unsigned>(tiles), kThreads, 0, s>>>(d_score, d_target, width, capacity, ws,
-                                                                     d_out);
-  return static_cast<int>(cudaGetLastError());
+                                  size_t workspace_bytes, hsi_stream_t stream) {
+  hsi_detect_job j;
+  j.score = d_score;
+  j.target = d_target;
+  j.height = height;
+  j.width = width;
+  j.threshold = threshold;
+  j.nms_radius = nms_radius;
+  j.polarity = polarity;
+  j.capacity = capacity;
+  j.out = d_out;
+  j.count = d_count;
+  return run_batch(&j, 1, d_workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" HSI_API int hsi_detect_batch(const hsi_detect_job* jobs, int num_jobs, void* d_workspace,
+                                        size_t workspace_bytes, hsi_stream_t stream) {
+  return run_batch(jobs, num_jobs, d_workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
 }

@@ -34,13 +34,15 @@ constexpr int kFiltersPerPass = HSI_MAX_FILTERS_PER_PASS;
 
 template <typename T>
 struct CubeTraits;
+// Stage ring depth: with two consumer warpgroups two CTAs fit per SM, and
+// 12 stages per SM keep ~190 KB of each SM's reads in flight.
 template <>
 struct CubeTraits<float> {
-  static constexpr int kStages = 4;
+  static constexpr int kStages = 6;
 };
 template <>
 struct CubeTraits<__half> {
-  static constexpr int kStages = 6;
+  static constexpr int kStages = 10;
 };
 
 struct ScoreParams {
@@ -108,7 +110,7 @@ __host__ __device__ inline SmemLayout smem_layout(int groups, int max_bands, int
   l.stage_bytes = static_cast<size_t>(kStageBands) * kTile * sizeof(T);
   size_t off = l.stage_bytes * CubeTraits<T>::kStages;
   l.filt_off = off;
-  off += static_cast<size_t>(groups) * max_bands * kg * sizeof(float);
+  off += static_cast<size_t>(groups) * max_bands * kg * 2 * sizeof(float);
   l.scale_off = off;
   off += static_cast<size_t>(groups) * kFiltersPerPass * sizeof(float);
   off = (off + 15) & ~static_cast<size_t>(15);
@@ -120,60 +122,54 @@ __host__ __device__ inline SmemLayout smem_layout(int groups, int max_bands, int
   return l;
 }
 
-// Accumulate one stage (nb bands) of this thread's 4 pixels against KG filters.
+// Packed FP32 FMA on sm_100: two lanes per instruction, d = a * b + c.
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;"
+      : "=l"(r)
+      : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)),
+        "l"(*reinterpret_cast<unsigned long long*>(&c)));
+  return *reinterpret_cast<float2*>(&r);
+}
+
+// Accumulate one stage (nb bands) of this thread's 4 pixels against KG
+// filters.  Pixels are held as pairs (p0,p1), (p2,p3); the filter bank is
+// stored duplicated, (f,f), so a 128-bit shared load yields two filters ready
+// for the packed FMA.
 template <typename T, int KG, bool kNorm>
-__device__ __forceinline__ void consume_stage(const T* stage, const float* filt, int nb, int tid,
-                                              float (&acc)[KG][kPPT], float (&nrm)[kPPT]) {
-  {
-    const T* src = stage + tid * kPPT;
-    if (nb == kStageBands) {
+__device__ __forceinline__ void consume_stage(const T* stage, const float* filt2, int nb, int tid,
+                                              float2 (&acc)[KG][2], float2 (&nrm)[2]) {
+  const T* src = stage + tid * kPPT;
+  auto band = [&](int i) {
+    float v[kPPT];
+    load4<T>(src + i * kTile, v);
+    const float2 v01 = make_float2(v[0], v[1]), v23 = make_float2(v[2], v[3]);
+    if constexpr (kNorm) {
+      nrm[0] = ffma2(v01, v01, nrm[0]);
+      nrm[1] = ffma2(v23, v23, nrm[1]);
+    }
+    const float* fr = filt2 + i * KG * 2;
+    if constexpr (KG >= 2) {
 #pragma unroll
-      for (int i = 0; i < kStageBands; ++i) {
-        float v[kPPT];
-        load4<T>(src + i * kTile, v);
-        const float* fr = filt + i * KG;
-        if constexpr (kNorm) {
-#pragma unroll
-          for (int j = 0; j < kPPT; ++j) nrm[j] = fmaf(v[j], v[j], nrm[j]);
-        }
-        if constexpr (KG >= 4) {
-#pragma unroll
-          for (int k = 0; k < KG; k += 4) {
-            const float4 f = ld_shared_f4(fr + k);
-#pragma unroll
-            for (int j = 0; j < kPPT; ++j) {
-              acc[k + 0][j] = fmaf(f.x, v[j], acc[k + 0][j]);
-              acc[k + 1][j] = fmaf(f.y, v[j], acc[k + 1][j]);
-              acc[k + 2][j] = fmaf(f.z, v[j], acc[k + 2][j]);
-              acc[k + 3][j] = fmaf(f.w, v[j], acc[k + 3][j]);
-            }
-          }
-        } else {
-#pragma unroll
-          for (int k = 0; k < KG; ++k) {
-            const float f = fr[k];
-#pragma unroll
-            for (int j = 0; j < kPPT; ++j) acc[k][j] = fmaf(f, v[j], acc[k][j]);
-          }
-        }
+      for (int k = 0; k < KG; k += 2) {
+        const float4 f = ld_shared_f4(fr + 2 * k);  // (f_k, f_k, f_k+1, f_k+1)
+        const float2 fa = make_float2(f.x, f.y), fb = make_float2(f.z, f.w);
+        acc[k][0] = ffma2(v01, fa, acc[k][0]);
+        acc[k][1] = ffma2(v23, fa, acc[k][1]);
+        acc[k + 1][0] = ffma2(v01, fb, acc[k + 1][0]);
+        acc[k + 1][1] = ffma2(v23, fb, acc[k + 1][1]);
       }
     } else {
-      for (int i = 0; i < nb; ++i) {
-        float v[kPPT];
-        load4<T>(src + i * kTile, v);
-        const float* fr = filt + i * KG;
-        if constexpr (kNorm) {
-#pragma unroll
-          for (int j = 0; j < kPPT; ++j) nrm[j] = fmaf(v[j], v[j], nrm[j]);
-        }
-#pragma unroll
-        for (int k = 0; k < KG; ++k) {
-          const float f = fr[k];
-#pragma unroll
-          for (int j = 0; j < kPPT; ++j) acc[k][j] = fmaf(f, v[j], acc[k][j]);
-        }
-      }
+      const float2 fa = *reinterpret_cast<const float2*>(fr);
+      acc[0][0] = ffma2(v01, fa, acc[0][0]);
+      acc[0][1] = ffma2(v23, fa, acc[0][1]);
     }
+  };
+  if (nb == kStageBands) {
+#pragma unroll
+    for (int i = 0; i < kStageBands; ++i) band(i);
+  } else {
+    for (int i = 0; i < nb; ++i) band(i);
   }
 }
 
@@ -183,7 +179,9 @@ __device__ __forceinline__ void store4(float* dst, const float v[kPPT], int vali
   if (vec && valid == kPPT) {
     *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
   } else {
-    for (int j = 0; j < valid; ++j) dst[j] = v[j];
+#pragma unroll
+    for (int j = 0; j < kPPT; ++j)
+      if (j < valid) dst[j] = v[j];
   }
 }
 
@@ -191,7 +189,9 @@ __device__ __forceinline__ void store4i(int32_t* dst, const int32_t v[kPPT], int
   if (vec && valid == kPPT) {
     *reinterpret_cast<int4*>(dst) = make_int4(v[0], v[1], v[2], v[3]);
   } else {
-    for (int j = 0; j < valid; ++j) dst[j] = v[j];
+#pragma unroll
+    for (int j = 0; j < kPPT; ++j)
+      if (j < valid) dst[j] = v[j];
   }
 }
 
@@ -202,8 +202,15 @@ __device__ __forceinline__ bool aligned16(const void* p) {
 // SAM epilogue for one thread's 4 pixels starting at frame pixel p.
 template <int KG>
 __device__ void sam_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, int valid,
-                             const float (&acc)[KG][kPPT], const float (&nrm)[kPPT],
-                             const float* scale) {
+                             const float2 (&acc2)[KG][2], const float2 (&nrm2)[2], const float* scale) {
+  float acc[KG][kPPT], nrm[kPPT] = {nrm2[0].x, nrm2[0].y, nrm2[1].x, nrm2[1].y};
+#pragma unroll
+  for (int k = 0; k < KG; ++k) {
+    acc[k][0] = acc2[k][0].x;
+    acc[k][1] = acc2[k][0].y;
+    acc[k][2] = acc2[k][1].x;
+    acc[k][3] = acc2[k][1].y;
+  }
   {
     const bool first = pass == 0;
     const bool last = pass_count(F.num_sam, pass + 1) == 0;
@@ -217,7 +224,9 @@ __device__ void sam_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, i
       best_t[j] = -1;
     }
     if (!first) {
-      for (int j = 0; j < valid; ++j) {
+#pragma unroll
+      for (int j = 0; j < kPPT; ++j) {
+        if (j >= valid) continue;
         if (F.sam_best) best[j] = F.sam_best[p + j];
         if (F.sam_best_target) best_t[j] = F.sam_best_target[p + j];
       }
@@ -255,7 +264,15 @@ __device__ void sam_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, i
 
 template <int KG>
 __device__ void cem_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, int valid,
-                             const float (&acc)[KG][kPPT]) {
+                             const float2 (&acc2)[KG][2]) {
+  float acc[KG][kPPT];
+#pragma unroll
+  for (int k = 0; k < KG; ++k) {
+    acc[k][0] = acc2[k][0].x;
+    acc[k][1] = acc2[k][0].y;
+    acc[k][2] = acc2[k][1].x;
+    acc[k][3] = acc2[k][1].y;
+  }
   {
     const bool first = pass == 0;
     const int t0 = pass * kFiltersPerPass;
@@ -267,7 +284,9 @@ __device__ void cem_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, i
       best_t[j] = -1;
     }
     if (!first) {
-      for (int j = 0; j < valid; ++j) {
+#pragma unroll
+      for (int j = 0; j < kPPT; ++j) {
+        if (j >= valid) continue;
         if (F.cem_best) best[j] = F.cem_best[p + j];
         if (F.cem_best_target) best_t[j] = F.cem_best_target[p + j];
       }
@@ -316,7 +335,9 @@ __device__ __forceinline__ void consumer_loop(const ScoreParams& prm, const int*
       const int t0 = prm.pass * kFiltersPerPass;
       for (int i = tid; i < B * KG; i += kGroupThreads) {
         const int b = i / KG, k = i % KG;
-        filt[i] = k < n_f ? src[static_cast<int64_t>(t0 + k) * B + b] : 0.0f;
+        const float v = k < n_f ? src[static_cast<int64_t>(t0 + k) * B + b] : 0.0f;
+        filt[2 * i] = v;
+        filt[2 * i + 1] = v;
       }
       if (kSam && tid < kFiltersPerPass) {
         const float nrm = tid < n_f ? F.sam_norms[t0 + tid] : 0.0f;
@@ -329,14 +350,10 @@ __device__ __forceinline__ void consumer_loop(const ScoreParams& prm, const int*
     const int64_t p0 = static_cast<int64_t>(tile - prefix[f]) * kTile;
     const bool active = n_f > 0;
 
-    float acc[KG][kPPT];
-    float nrm[kPPT];
+    float2 acc[KG][2];
+    float2 nrm[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
 #pragma unroll
-    for (int k = 0; k < KG; ++k)
-#pragma unroll
-      for (int j = 0; j < kPPT; ++j) acc[k][j] = 0.0f;
-#pragma unroll
-    for (int j = 0; j < kPPT; ++j) nrm[j] = 0.0f;
+    for (int k = 0; k < KG; ++k) acc[k][0] = acc[k][1] = make_float2(0.0f, 0.0f);
 
     for (int b0 = 0; b0 < B; b0 += kStageBands) {
       const int nb = B - b0 < kStageBands ? B - b0 : kStageBands;
@@ -349,7 +366,7 @@ __device__ __forceinline__ void consumer_loop(const ScoreParams& prm, const int*
       }
       if (active && !aborted) {
         const T* stage = reinterpret_cast<const T*>(smem + slot * stage_bytes);
-        consume_stage<T, KG, kSam>(stage, filt + b0 * KG, nb, tid, acc, nrm);
+        consume_stage<T, KG, kSam>(stage, filt + 2 * b0 * KG, nb, tid, acc, nrm);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[slot]);
@@ -463,7 +480,7 @@ __global__ void __launch_bounds__(((KS > 0) + (KC > 0)) * kGroupThreads + 32)
   // ---------------- consumer warpgroups ----------------
   const int group = warp / (kGroupThreads / 32);  // 0: SAM if KS > 0, else CEM; 1: CEM
   const int tid = threadIdx.x - group * kGroupThreads;
-  float* filt = reinterpret_cast<float*>(smem + L.filt_off) + static_cast<size_t>(group) * max_bands * kKG;
+  float* filt = reinterpret_cast<float*>(smem + L.filt_off) + static_cast<size_t>(group) * max_bands * kKG * 2;
   float* scale = reinterpret_cast<float*>(smem + L.scale_off) + group * kFiltersPerPass;
   if constexpr (KS > 0) {
     if (group == 0) {

@@ -14,7 +14,7 @@
 // exactly.  So:
 //   d = x - r (r: per-band reference near the mean, as the reference's shifted
 //   accumulation, include/hsi/linalg.hpp:53-90), fixed point
-//   q = rint(d * 2^e_b) with |q| < 2^23 (e_b from a subsample with 4x headroom;
+//   q = rint(d * 2^e_b) with |q| < 2^22 (e_b from a subsample with 4x headroom;
 //   an overflow re-runs the pass with the observed range), balanced signed
 //   8-bit limbs q = L0*2^16 + L1*2^8 + L2, and four exact INT32 accumulators
 //     A0 = sum L0 L0^T,  A1 = sum L0 L1^T,  A2 = sum (L1 L1^T + 2 L0 L2^T),
@@ -29,12 +29,13 @@
 //   pixel count.  Partial sums of all CTAs are reduced in a fixed order and
 //   rebuilt as raw moments in FP64 (src/linalg.cpp:81-103).
 //
-// Kernel roles (one CTA per SM, 14 warps):
-//   warp 0       TMA producer: two 64-pixel x 128-band boxes per K-block
+// Kernel roles (one CTA per SM, 22 warps):
+//   warp 0       TMA producer: 64-pixel x 128-band boxes, two per K-block,
+//                into a 4-deep ring (3 boxes in flight while one converts)
 //   warp 1       TMEM allocator + single-thread MMA issuer
-//   warps 2-9    converters: FP32 tile -> INT8 limbs L0, L1, L2 in the UMMA
+//   warps 2-17   converters: FP32 tile -> INT8 limbs L0, L1, L2 in the UMMA
 //                128-byte-swizzled K-major layout; per-band |d| maxima
-//   warps 10-13  epilogue: INT32 TMEM accumulators -> FP64 partials (once per
+//   warps 18-21  epilogue: INT32 TMEM accumulators -> FP64 partials (once per
 //                32768-pixel chunk, i.e. once per frame at typical sizes)
 // TMEM: columns [0,128) A0, [128,256) A1, [256,384) A2, [384,512) A3.
 #include <cuda_bf16.h>
@@ -50,28 +51,29 @@ constexpr int kBoxPx = 64;       // pixels per TMA box
 constexpr int kChunkKB = 256;    // K-blocks per INT32 chunk: 32768 px, no overflow
 constexpr int kRows = 128;       // band rows of the GEMM (bands + ones row)
 constexpr int kOpStages = 2;
-constexpr int kConvWarps = 8;
+constexpr int kConvWarps = 16;
 constexpr int kEpiWarps = 4;
 constexpr int kWarpTma = 0;
 constexpr int kWarpMma = 1;
 constexpr int kWarpConv0 = 2;
 constexpr int kWarpEpi0 = kWarpConv0 + kConvWarps;
-constexpr int kThreads = (kWarpEpi0 + kEpiWarps) * 32;  // 448
+constexpr int kThreads = (kWarpEpi0 + kEpiWarps) * 32;  // 704
 constexpr int kLimbBytes = kRows * kKB;                 // 16 KB per limb tile
 constexpr uint32_t kTmemCols = 512;
 constexpr int kMaxTensorBands = kRows - 1;  // 127: room for the ones row
 constexpr int kMaxCtas = 160;
 constexpr int64_t kTensorMinPixels = 32768;
-constexpr int kQMax = (1 << 23) - (1 << 16) - 1;
+constexpr int kQMax = (1 << 22) - (1 << 16);  // |q| bound of the FMA rounding trick
 constexpr int kOnesExp = 16;  // the ones row holds q = 2^16
 
+// Input stages hold one TMA box (half a K-block: 64 pixels x 128 bands).
 template <typename T>
 constexpr int in_stages() {
-  return sizeof(T) == 4 ? 2 : 4;
+  return sizeof(T) == 4 ? 4 : 8;
 }
 template <typename T>
 constexpr int in_tile_bytes() {
-  return kRows * kKB * static_cast<int>(sizeof(T));
+  return kRows * kBoxPx * static_cast<int>(sizeof(T));
 }
 
 struct StatsSmem {
@@ -91,7 +93,7 @@ __host__ __device__ inline StatsSmem stats_smem() {
   s.scale_off = off;
   off += kRows * sizeof(float);
   s.bar_off = off;
-  off += (2 * 4 + 2 * kOpStages + 3) * sizeof(uint64_t);
+  off += (2 * 8 + 2 * kOpStages + 3) * sizeof(uint64_t);
   s.slot_off = off;
   off += 16;
   s.total = off + 1024;  // slack to align the dynamic base to 1024
@@ -126,6 +128,11 @@ struct StatsState {
   int flags;                          // bit 0: a q was clamped; bit 1: the re-run is armed
   int pad[3];
   unsigned long long l2sq[HSI_MAX_BANDS + 1];  // exact sum of L2^2 per band
+  // subsample pass (cleared by a memset before it)
+  double sub_sum[HSI_MAX_BANDS + 1];
+  double sub_cnt[HSI_MAX_BANDS + 1];
+  int sub_lo[HSI_MAX_BANDS + 1];  // float_order of the minimum
+  int sub_hi[HSI_MAX_BANDS + 1];
 };
 
 struct StatsArgs {
@@ -160,8 +167,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   const StatsSmem L = stats_smem<T>();
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar_off);
   uint64_t* in_full = bars;
-  uint64_t* in_empty = in_full + 4;
-  uint64_t* op_full = in_empty + 4;
+  uint64_t* in_empty = in_full + 8;
+  uint64_t* op_full = in_empty + 8;
   uint64_t* op_empty = op_full + kOpStages;
   uint64_t* acc_full = op_empty + kOpStages;
   uint64_t* acc_empty = acc_full + 1;
@@ -211,7 +218,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (lane == 0) {
       prefetch_tensormap(&cube_map);
       uint32_t pending = 0, parity = 0;
-      for (int i = 0; i < n; ++i) {
+      for (int i = 0; i < 2 * n; ++i) {
         const int s = i % kInStages;
         const uint32_t ph = (i / kInStages) & 1u;
         if (*abort_flag || !mbar_wait(&in_empty[s], ph ^ 1u)) {
@@ -221,9 +228,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         unsigned char* dst = smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>();
         mbar_arrive_expect_tx(&in_full[s], in_tile_bytes<T>());
-        const int x = static_cast<int>((kb0 + i) * kKB);
-        tma_load_2d(dst, &cube_map, x, 0, &in_full[s]);
-        tma_load_2d(dst + in_tile_bytes<T>() / 2, &cube_map, x + kBoxPx, 0, &in_full[s]);
+        tma_load_2d(dst, &cube_map, static_cast<int>(kb0 * kKB + static_cast<int64_t>(i) * kBoxPx), 0, &in_full[s]);
         pending |= 1u << s;
         parity = (parity & ~(1u << s)) | (ph << s);
       }
@@ -280,89 +285,108 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp < kWarpEpi0) {
     // ---------------- converters ----------------
-    // warp cw: bands cw + 8t (t < 16); lane: pixels 4*lane .. 4*lane + 3
+    // Each input stage is half a K-block (64 pixels).  Warp cw owns 4 band
+    // pairs (b, b+4) -- lanes 0-15 the first band, 16-31 the second, 4 pixels
+    // per lane -- so one store instruction covers two rows whose swizzled
+    // chunks never share a bank.
+    // q = rint((x - r) 2^e) comes out of one FMA: adding 1.5*2^23 leaves
+    // rint(q) in the low mantissa bits (|q| < 2^22), and w = q + 0x8080 has
+    // the balanced limbs as its bytes (low two XOR 0x80, third as is).
     const int cw = warp - kWarpConv0;
-    constexpr int kBandsPerWarp = kRows / kConvWarps;
-    float rr[kBandsPerWarp], sc[kBandsPerWarp], mx[kBandsPerWarp];
-    uint32_t l2sq[kBandsPerWarp];
+    constexpr int kSlots = kRows / 2 / kConvWarps;  // 4 band pairs per warp
+    constexpr float kMagic = 12582912.0f;          // 1.5 * 2^23
+    const int sub = lane >> 4, lp = (lane & 15) * 4;  // which band of the pair; pixel in the box
+    int band[kSlots];
+    float sc[kSlots], off[kSlots], xlo[kSlots], xhi[kSlots];
+    int l2sq[kSlots];
 #pragma unroll
-    for (int t = 0; t < kBandsPerWarp; ++t) {
-      rr[t] = shift[cw + kConvWarps * t];
-      sc[t] = scale[cw + kConvWarps * t];
-      mx[t] = 0.0f;
-      l2sq[t] = 0u;
+    for (int t = 0; t < kSlots; ++t) {
+      const int pair = cw + kConvWarps * t;          // 0..63
+      const int b = (pair >> 2) * 8 + (pair & 3) + 4 * sub;
+      band[t] = b;
+      sc[t] = scale[b];
+      off[t] = kMagic - shift[b] * scale[b];  // exact: r sits on the 2^-e grid
+      xlo[t] = INFINITY;
+      xhi[t] = -INFINITY;
+      l2sq[t] = 0;
     }
-    bool aborted = false, clamped = false;
-    const int half = lane >> 4, hp = (lane & 15) * 4;  // box half and pixel within it
-    for (int i = 0; i < n; ++i) {
-      const int s = i % kInStages, so = i % kOpStages;
-      if (!aborted && (!mbar_wait(&in_full[s], (i / kInStages) & 1u) ||
-                       !mbar_wait(&op_empty[so], ((i / kOpStages) & 1u) ^ 1u))) {
+    const int wbias = __float_as_int(kMagic) - 0x8080;
+    bool aborted = false;
+    for (int j = 0; j < 2 * n; ++j) {
+      const int s = j % kInStages, i = j >> 1, half = j & 1, so = i % kOpStages;
+      if (!aborted && (!mbar_wait(&in_full[s], (j / kInStages) & 1u) ||
+                       (half == 0 && !mbar_wait(&op_empty[so], ((i / kOpStages) & 1u) ^ 1u)))) {
         record_error(args.status, HSI_E_TIMEOUT);
         *abort_flag = 1;
         aborted = true;
       }
       if (aborted) break;
-      const T* in = reinterpret_cast<const T*>(smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>()) +
-                    half * (kRows * kBoxPx);
+      const T* in = reinterpret_cast<const T*>(smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>());
       unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kLimbBytes;
-      const int64_t gp = (kb0 + i) * kKB + 4 * lane;
+      const int64_t gp = (kb0 + i) * kKB + half * kBoxPx + lp;
       const int nvalid = gp >= P ? 0 : (P - gp >= 4 ? 4 : static_cast<int>(P - gp));
 #pragma unroll
-      for (int t = 0; t < kBandsPerWarp; ++t) {
-        const int b = cw + kConvWarps * t;
-        int q[4] = {0, 0, 0, 0};
+      for (int t = 0; t < kSlots; ++t) {
+        const int b = band[t];
+        int w[4] = {0x8080, 0x8080, 0x8080, 0x8080};  // q = 0
         if (b < B) {
-          const float4 x = load4f<T>(in + b * kBoxPx + hp);
+          const float4 x = load4f<T>(in + b * kBoxPx + lp);
           const float xv[4] = {x.x, x.y, x.z, x.w};
+          // fully unrolled with a predicate: a loop bounded by nvalid would
+          // index w[] dynamically and move it to local memory
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             if (e < nvalid) {
-              const float d = xv[e] - rr[t];
-              mx[t] = fmaxf(mx[t], fabsf(d));
-              int v = __float2int_rn(d * sc[t]);
-              if (v > kQMax || v < -kQMax || !(fabsf(d * sc[t]) <= static_cast<float>(kQMax))) {
-                clamped = true;
-                v = v > 0 ? kQMax : -kQMax;
-              }
-              q[e] = v;
+              xlo[t] = fminf(xlo[t], xv[e]);
+              xhi[t] = fmaxf(xhi[t], xv[e]);
+              w[e] = __float_as_int(fmaf(xv[e], sc[t], off[t])) - wbias;
             }
           }
         } else if (b == B) {
 #pragma unroll
-          for (int e = 0; e < 4; ++e) q[e] = e < nvalid ? (1 << kOnesExp) : 0;
+          for (int e = 0; e < 4; ++e) w[e] = e < nvalid ? (1 << kOnesExp) + 0x8080 : 0x8080;
         }
-        int l0[4], l1[4], l2[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          limbs(q[e], l0[e], l1[e], l2[e]);
-          l2sq[t] += static_cast<uint32_t>(l2[e] * l2[e]);
-        }
-        const uint32_t off = sw128_byte(b, 4 * lane);
-        *reinterpret_cast<uint32_t*>(op + off) = pack4(l0[0], l0[1], l0[2], l0[3]);
-        *reinterpret_cast<uint32_t*>(op + kLimbBytes + off) = pack4(l1[0], l1[1], l1[2], l1[3]);
-        *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + off) = pack4(l2[0], l2[1], l2[2], l2[3]);
+        const uint32_t p01 = __byte_perm(w[0], w[1], 0x5140), p23 = __byte_perm(w[2], w[3], 0x5140);
+        const uint32_t h01 = __byte_perm(w[0], w[1], 0x7362), h23 = __byte_perm(w[2], w[3], 0x7362);
+        const uint32_t l2 = __byte_perm(p01, p23, 0x5410) ^ 0x80808080u;
+        const uint32_t l1 = __byte_perm(p01, p23, 0x7632) ^ 0x80808080u;
+        const uint32_t l0 = __byte_perm(h01, h23, 0x5410);
+        l2sq[t] = __dp4a(static_cast<int>(l2), static_cast<int>(l2), l2sq[t]);
+        const uint32_t o = sw128_byte(b, half * kBoxPx + lp);
+        *reinterpret_cast<uint32_t*>(op + o) = l0;
+        *reinterpret_cast<uint32_t*>(op + kLimbBytes + o) = l1;
+        *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + o) = l2;
       }
-      fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0) {
-        mbar_arrive(&in_empty[s]);
-        mbar_arrive(&op_full[so]);
+      if (lane == 0) mbar_arrive(&in_empty[s]);
+      if (half == 1) {
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&op_full[so]);
       }
     }
-    // per-band |d| maxima and the clamp flag, for the re-run and for the
-    // whitening pass's fixed-point range
+    // per band: |x - r| range (for the re-run and for the whitening pass), the
+    // clamp check, and the exact sum of L2^2 (reduced over the 16 lanes that
+    // share the band)
+    bool clamped = false;
 #pragma unroll
-    for (int t = 0; t < kBandsPerWarp; ++t) {
-      float m = mx[t];
+    for (int t = 0; t < kSlots; ++t) {
+      float lo = xlo[t], hi = xhi[t];
+      unsigned long long sq = static_cast<unsigned int>(l2sq[t]);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-      const int b = cw + kConvWarps * t;
-      if (lane == 0 && b < B) atomicMax(&args.state->maxdev_bits[b], __float_as_int(m));
-      unsigned long long sq = l2sq[t];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-      if (lane == 0 && b < B) atomicAdd(&args.state->l2sq[b], sq);
+      for (int o = 8; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        sq += __shfl_xor_sync(0xffffffffu, sq, o);
+      }
+      const int b = band[t];
+      const float r = shift[b];
+      const float m = hi >= lo ? fmaxf(hi - r, r - lo) : 0.0f;
+      if (b < B && !(m * sc[t] <= static_cast<float>(kQMax))) clamped = true;
+      if ((lane & 15) == 0 && b < B) {
+        atomicMax(&args.state->maxdev_bits[b], __float_as_int(m));
+        atomicAdd(&args.state->l2sq[b], sq);
+      }
     }
     if (__any_sync(0xffffffffu, clamped) && lane == 0) atomicOr(&args.state->flags, 1);
   } else {
@@ -413,41 +437,54 @@ __global__ void __launch_bounds__(kThreads, 1)
 // ---------------------------------------------------------------------------
 // Reference point and fixed-point scale per band from a regular subsample
 // (every 16th run of 64 pixels on large frames): r = subsample mean, e such
-// that the subsample's largest |x - r| maps to 2^21 (4x headroom below 2^23).
+// that the subsample's largest |x - r| maps to 2^20 (4x headroom below 2^22).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int scale_exp_for(float maxdev) {
-  if (!(maxdev > 0.0f)) return 21;
+  if (!(maxdev > 0.0f)) return 20;
   int e;
   frexpf(maxdev, &e);  // maxdev in [2^(e-1), 2^e)
-  int k = 21 - e;      // maxdev * 2^k < 2^21
+  int k = 20 - e;      // maxdev * 2^k < 2^20
   return k < -120 ? -120 : (k > 120 ? 120 : k);
 }
 
+// Monotone map of a float onto a signed int, so atomicMin/atomicMax order
+// floats of either sign.
+__device__ __forceinline__ int float_order(float v) {
+  const int i = __float_as_int(v);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float order_float(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+constexpr int kShiftSplit = 16;  // blocks per band of the subsample pass
+
+__global__ void shift_init_kernel(StatsState* st) {
+  for (int b = threadIdx.x; b <= HSI_MAX_BANDS; b += blockDim.x) {
+    st->sub_sum[b] = 0.0;
+    st->sub_cnt[b] = 0.0;
+    st->sub_lo[b] = 0x7fffffff;
+    st->sub_hi[b] = static_cast<int>(0x80000000u);
+  }
+}
+
+// Subsample statistics, spread over (bands x kShiftSplit) blocks: runs of 64
+// pixels, every 16th run on large frames; partial sums land in the state with
+// atomics (the state is cleared by a memset first).
 template <typename T>
-__global__ void __launch_bounds__(256) shift_kernel(const T* __restrict__ cube, int64_t pixels, int64_t stride,
-                                                    int bands, const float* __restrict__ given, StatsState* st) {
+__global__ void __launch_bounds__(256) shift_partial_kernel(const T* __restrict__ cube, int64_t pixels,
+                                                            int64_t stride, int bands, StatsState* st) {
   const int b = blockIdx.x;
-  if (threadIdx.x == 0) {
-    if (b == 0) st->flags = 0;
-    st->maxdev_bits[b] = 0;
-    st->l2sq[b] = 0ull;
-  }
-  if (b >= bands) {
-    if (threadIdx.x == 0) {
-      st->shift[b] = 0.0f;
-      st->scale_exp[b] = b == bands ? kOnesExp : 0;
-    }
-    return;
-  }
-  __shared__ double s_sum[256];
-  __shared__ double s_cnt[256];
-  __shared__ float s_lo[256], s_hi[256];
+  if (b >= bands) return;
+  __shared__ double s_sum[8], s_cnt[8];
+  __shared__ int s_lo[8], s_hi[8];
   const T* plane = cube + static_cast<int64_t>(b) * stride;
   const int64_t runs = div_up<int64_t>(pixels, 64);
   const int64_t step = runs > 4096 ? 16 : 1;
+  const int64_t sampled = div_up<int64_t>(runs, step);
+  const int64_t r0 = sampled * blockIdx.y / kShiftSplit, r1 = sampled * (blockIdx.y + 1) / kShiftSplit;
   double sum = 0.0, cnt = 0.0;
   float lo = INFINITY, hi = -INFINITY;
-  for (int64_t run = threadIdx.x / 64; run * step < runs; run += blockDim.x / 64) {
+#pragma unroll 4
+  for (int64_t run = r0 + threadIdx.x / 64; run < r1; run += blockDim.x / 64) {
     const int64_t p = run * step * 64 + (threadIdx.x & 63);
     if (p < pixels) {
       const float v = static_cast<float>(plane[p]);
@@ -457,30 +494,66 @@ __global__ void __launch_bounds__(256) shift_kernel(const T* __restrict__ cube, 
       hi = fmaxf(hi, v);
     }
   }
-  s_sum[threadIdx.x] = sum;
-  s_cnt[threadIdx.x] = cnt;
-  s_lo[threadIdx.x] = lo;
-  s_hi[threadIdx.x] = hi;
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) {
-      s_sum[threadIdx.x] += s_sum[threadIdx.x + w];
-      s_cnt[threadIdx.x] += s_cnt[threadIdx.x + w];
-      s_lo[threadIdx.x] = fminf(s_lo[threadIdx.x], s_lo[threadIdx.x + w]);
-      s_hi[threadIdx.x] = fmaxf(s_hi[threadIdx.x], s_hi[threadIdx.x + w]);
-    }
-    __syncthreads();
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
   }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    s_sum[warp] = sum;
+    s_cnt[warp] = cnt;
+    s_lo[warp] = float_order(lo);
+    s_hi[warp] = float_order(hi);
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    float r = given ? given[b] : (s_cnt[0] > 0.0 ? static_cast<float>(s_sum[0] / s_cnt[0]) : 0.0f);
-    const float dev = fmaxf(fabsf(s_hi[0] - r), fabsf(s_lo[0] - r));
-    const int e = scale_exp_for(dev * 1.0000001f);
-    // r on the fixed-point grid: inputs that are themselves multiples of 2^-e
-    // (FP16 cubes, quantised sensors) then convert to q without rounding
+    double ts = 0.0, tc = 0.0;
+    int tl = s_lo[0], th = s_hi[0];
+    for (int w = 0; w < 8; ++w) {
+      ts += s_sum[w];
+      tc += s_cnt[w];
+      tl = min(tl, s_lo[w]);
+      th = max(th, s_hi[w]);
+    }
+    if (tc > 0.0) {
+      atomicAdd(&st->sub_sum[b], ts);
+      atomicAdd(&st->sub_cnt[b], tc);
+      atomicMin(&st->sub_lo[b], tl);
+      atomicMax(&st->sub_hi[b], th);
+    }
+  }
+}
+
+// r = subsample mean (or the caller's reference), e such that the subsample's
+// largest |x - r| maps to 2^20 (4x headroom below 2^22), r snapped to the
+// 2^-e grid so that inputs on that grid (FP16 cubes) convert exactly.
+__global__ void __launch_bounds__(256) shift_finalize_kernel(int bands, const float* __restrict__ given,
+                                                             StatsState* st) {
+  for (int b = threadIdx.x; b <= HSI_MAX_BANDS; b += blockDim.x) {
+    st->maxdev_bits[b] = 0;
+    st->l2sq[b] = 0ull;
+    if (b > bands) {
+      st->shift[b] = 0.0f;
+      st->scale_exp[b] = 0;
+      continue;
+    }
+    if (b == bands) {
+      st->shift[b] = 0.0f;
+      st->scale_exp[b] = kOnesExp;
+      continue;
+    }
+    const double c = st->sub_cnt[b];
+    float r = given ? given[b] : (c > 0.0 ? static_cast<float>(st->sub_sum[b] / c) : 0.0f);
+    const float lo = c > 0.0 ? order_float(st->sub_lo[b]) : r, hi = c > 0.0 ? order_float(st->sub_hi[b]) : r;
+    const int e = scale_exp_for(fmaxf(fabsf(hi - r), fabsf(lo - r)) * 1.0000001f);
     r = ldexpf(rintf(ldexpf(r, e)), -e);
     st->shift[b] = r;
     st->scale_exp[b] = e;
   }
+  if (threadIdx.x == 0) st->flags = 0;
 }
 
 // After the first GEMM: if a value was clamped, take the range the GEMM
@@ -489,7 +562,10 @@ __global__ void rescale_kernel(int bands, StatsState* st) {
   if (!(st->flags & 1)) return;
   for (int b = threadIdx.x; b < bands; b += blockDim.x) {
     const float dev = __int_as_float(st->maxdev_bits[b]);
-    st->scale_exp[b] = scale_exp_for(dev * 1.0000001f) + 2;  // observed max -> 2^23 range
+    const int e = scale_exp_for(dev * 1.0000001f) + 1;  // observed max -> below 2^21
+    st->scale_exp[b] = e;
+    // keep r on the (coarser) new grid so r * 2^e stays an exact integer
+    st->shift[b] = ldexpf(rintf(ldexpf(st->shift[b], e)), -e);
     st->l2sq[b] = 0ull;  // recounted by the re-run
   }
   __syncthreads();
@@ -519,37 +595,36 @@ __global__ void __launch_bounds__(256) stats_reduce_kernel(const double* __restr
 // (moments_from_shifted, src/linalg.cpp:81-103).  fsum is column-major:
 // fsum[col * 128 + row] = F[row][col].  Output: sum[B], outer[B*B] (full,
 // symmetric), count.
-__global__ void __launch_bounds__(256) stats_finalize_kernel(const double* __restrict__ fsum,
+__global__ void __launch_bounds__(128) stats_finalize_kernel(const double* __restrict__ fsum,
                                                             const StatsState* __restrict__ st, int bands,
                                                             double* __restrict__ moments) {
+  // one block per row i of the output; every block rebuilds the first moments
   __shared__ double s1[kRows];
   __shared__ double r[kRows];
   __shared__ int ex[kRows];
   const int B = bands;
+  const int i = blockIdx.x;
   auto F = [&](int row, int col) { return fsum[static_cast<size_t>(col) * kRows + row]; };
   const double N = ldexp(F(B, B), -2 * kOnesExp);
-  for (int i = threadIdx.x; i < B; i += blockDim.x) {
-    ex[i] = st->scale_exp[i];
-    r[i] = static_cast<double>(st->shift[i]);
+  for (int j = threadIdx.x; j < B; j += blockDim.x) {
+    ex[j] = st->scale_exp[j];
+    r[j] = static_cast<double>(st->shift[j]);
+    s1[j] = ldexp(0.5 * (F(j, B) + F(B, j)), -(st->scale_exp[j] + kOnesExp));
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < B; i += blockDim.x) s1[i] = ldexp(0.5 * (F(i, B) + F(B, i)), -(ex[i] + kOnesExp));
-  __syncthreads();
-  double* sum = moments;
   double* outer = moments + B;
-  for (int i = threadIdx.x; i < B; i += blockDim.x) sum[i] = s1[i] + N * r[i];
-  // lower triangle, mirrored, so the matrix is exactly symmetric
-  for (int e = threadIdx.x; e < B * B; e += blockDim.x) {
-    const int i = e / B, j = e % B;
-    if (j > i) continue;
+  if (i == 0)
+    for (int j = threadIdx.x; j < B; j += blockDim.x) moments[j] = s1[j] + N * r[j];
+  // row i, columns j <= i, mirrored, so the matrix is exactly symmetric
+  for (int j = threadIdx.x; j <= i; j += blockDim.x) {
     double q = 0.5 * (F(i, j) + F(j, i));
     if (i == j) q += static_cast<double>(st->l2sq[i]);  // the weight-1 diagonal, exact
     const double s2 = ldexp(q, -(ex[i] + ex[j]));
     const double v = s2 + r[i] * s1[j] + s1[i] * r[j] + N * r[i] * r[j];
-    outer[e] = v;
-    outer[j * B + i] = v;
+    outer[static_cast<size_t>(i) * B + j] = v;
+    outer[static_cast<size_t>(j) * B + i] = v;
   }
-  if (threadIdx.x == 0) moments[B + B * B] = N;
+  if (i == 0 && threadIdx.x == 0) moments[B + B * B] = N;
 }
 
 // ---------------------------------------------------------------------------
@@ -748,6 +823,14 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
+template <typename T>
+void launch_shift(const void* cube, int64_t P, int64_t stride, int B, const float* reference, StatsState* st,
+                  cudaStream_t s) {
+  shift_init_kernel<<<1, 256, 0, s>>>(st);
+  shift_partial_kernel<T><<<dim3(B, kShiftSplit), 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, st);
+  shift_finalize_kernel<<<1, 256, 0, s>>>(B, reference, st);
+}
+
 // shift + scale -> GEMM -> (conditional) rescale + GEMM re-run -> reduce -> finalize
 template <typename T>
 int launch_tensor_stats(const void* cube, int64_t P, int B, int64_t stride, double* moments, const float* reference,
@@ -756,7 +839,7 @@ int launch_tensor_stats(const void* cube, int64_t P, int B, int64_t stride, doub
   const int rc = encode_cube_map(&map, cube, sizeof(T) == 4 ? HSI_F32 : HSI_F16, P, B, stride, kBoxPx, kRows);
   if (rc != HSI_OK) return rc;
   const StatsWorkspace w = carve(workspace, static_cast<size_t>(kMaxCtas) * kRows * kRows * sizeof(double));
-  shift_kernel<T><<<kRows, 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, reference, w.state);
+  launch_shift<T>(cube, P, stride, B, reference, w.state, s);
   const int64_t nkb = div_up<int64_t>(P, kKB);
   int grid = num_sms();
   if (grid > kMaxCtas) grid = kMaxCtas;
@@ -781,7 +864,7 @@ int launch_tensor_stats(const void* cube, int64_t P, int B, int64_t stride, doub
   a.conditional = 1;
   stats_gemm_kernel<T><<<grid, kThreads, L.total, s>>>(map, a);
   stats_reduce_kernel<<<kRows * kRows / 32, 256, 0, s>>>(w.partials, grid, w.fsum);
-  stats_finalize_kernel<<<1, 256, 0, s>>>(w.fsum, w.state, B, moments);
+  stats_finalize_kernel<<<B, 128, 0, s>>>(w.fsum, w.state, B, moments);
   return static_cast<int>(cudaGetLastError());
 }
 
@@ -791,7 +874,7 @@ int launch_simt_stats(const void* cube, int64_t P, int B, int64_t stride, double
   const int tiles = (B + 1 + kSimtTile - 1) / kSimtTile;
   const int n = tiles * kSimtTile;
   const StatsWorkspace w = carve(workspace, static_cast<size_t>(kSimtSlices) * n * n * sizeof(double));
-  shift_kernel<T><<<HSI_MAX_BANDS + 1, 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, reference, w.state);
+  launch_shift<T>(cube, P, stride, B, reference, w.state, s);
   const dim3 grid(kSimtSlices, tiles * (tiles + 1) / 2);
   stats_simt_kernel<T><<<grid, 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, w.state, w.partials,
                                            kSimtSlices);

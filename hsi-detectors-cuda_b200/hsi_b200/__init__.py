@@ -52,6 +52,16 @@ class Scene(C.Structure):
     ]
 
 
+class DetectJob(C.Structure):
+    """hsi_detect_job: one score map of a batched detection call (device pointers)."""
+
+    _fields_ = [
+        ("score", C.c_void_p), ("target", C.c_void_p), ("height", C.c_int32), ("width", C.c_int32),
+        ("threshold", C.c_float), ("nms_radius", C.c_int32), ("polarity", C.c_int32), ("capacity", C.c_int32),
+        ("out", C.c_void_p), ("count", C.c_void_p),
+    ]
+
+
 class Frame(C.Structure):
     """hsi_frame: one frame's cube, filter bank and output maps (device pointers)."""
 
@@ -102,6 +112,10 @@ def lib():
         L.hsi_detect_workspace_bytes.restype = C.c_size_t
         L.hsi_detect.argtypes = [vp, vp, i32, i32, C.c_float, i32, i32, i32, vp, vp, vp, C.c_size_t, vp]
         L.hsi_detect.restype = i32
+        L.hsi_detect_batch_workspace_bytes.argtypes = [C.POINTER(DetectJob), i32]
+        L.hsi_detect_batch_workspace_bytes.restype = C.c_size_t
+        L.hsi_detect_batch.argtypes = [C.POINTER(DetectJob), i32, vp, C.c_size_t, vp]
+        L.hsi_detect_batch.restype = i32
         _optional_symbols(L)
         _lib = L
     return _lib
@@ -279,6 +293,23 @@ def detect(score, target, height, width, threshold, nms_radius=2, polarity=LOWER
                            capacity, _ptr(out), _ptr(count), _ptr(workspace), workspace.numel(),
                            _stream(stream)), "hsi_detect")
     return count, out
+
+
+def detect_job(score, target, height, width, threshold, nms_radius, polarity, capacity, out, count) -> DetectJob:
+    return DetectJob(score.data_ptr(), None if target is None else target.data_ptr(), height, width,
+                     float(threshold), nms_radius, polarity, capacity, out.data_ptr(), count.data_ptr())
+
+
+def detect_batch_workspace_bytes(jobs) -> int:
+    arr = (DetectJob * len(jobs))(*jobs)
+    return lib().hsi_detect_batch_workspace_bytes(arr, len(jobs))
+
+
+def detect_batch(jobs, workspace, stream=None) -> None:
+    """Up to 64 maps in three launches; see hsi_detect_batch."""
+    arr = (DetectJob * len(jobs))(*jobs)
+    check(lib().hsi_detect_batch(arr, len(jobs), _ptr(workspace), workspace.numel(), _stream(stream)),
+          "hsi_detect_batch")
 
 
 def detections_to_numpy(count, out, capacity):

@@ -267,6 +267,26 @@ HSI_API int hsi_detect(const float* d_score, const int32_t* d_target, int height
                        hsi_detection* d_out, uint32_t* d_count, void* d_workspace,
                        size_t workspace_bytes, hsi_stream_t stream);
 
+/* The same for up to 64 score maps in three launches (one per stage for the
+ * whole batch).  Job descriptors live in host memory; the pointers in them
+ * are device pointers. */
+typedef struct hsi_detect_job {
+  const float* score;
+  const int32_t* target;     /* nullable */
+  int32_t height;
+  int32_t width;
+  float threshold;
+  int32_t nms_radius;
+  int32_t polarity;
+  int32_t capacity;
+  hsi_detection* out;
+  uint32_t* count;
+} hsi_detect_job;
+#define HSI_MAX_DETECT_JOBS 64
+HSI_API size_t hsi_detect_batch_workspace_bytes(const hsi_detect_job* jobs, int num_jobs);
+HSI_API int hsi_detect_batch(const hsi_detect_job* jobs, int num_jobs, void* d_workspace,
+                             size_t workspace_bytes, hsi_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -94,3 +94,29 @@ def test_workspace_is_checked(hsi):
     with pytest.raises(hsi.HsiError) as e:
         hsi.detect(s, None, 8, 8, 0.1, 0, 0, 16, workspace=small)
     assert e.value.status == hsi.E_WORKSPACE
+
+
+def test_batched_maps_match_single_calls(hsi, orc):
+    """Up to 64 maps of different sizes, radii and polarities in one call."""
+    rng = np.random.default_rng(77)
+    specs = [(37, 53, 0, False), (1, 1, 2, True), (64, 2100, 2, False), (300, 7, 4, True), (128, 128, 6, False),
+             (5, 5000, 1, True)]
+    jobs, keep = [], []
+    for (H, W, r, higher) in specs:
+        score = (rng.integers(0, 30, H * W) / 30.0).astype(np.float32)
+        target = rng.integers(0, 8, H * W).astype(np.int32)
+        s = torch.from_numpy(score).cuda()
+        t = torch.from_numpy(target).cuda()
+        out = torch.full((H * W + 1, 4), -1, dtype=torch.int32, device="cuda")
+        count = torch.zeros(1, dtype=torch.int32, device="cuda")
+        thr = 0.85 if higher else 0.15
+        jobs.append(hsi.detect_job(s, t, H, W, thr, r, 1 if higher else 0, H * W + 1, out, count))
+        keep.append((score, target, H, W, thr, r, higher, s, t, out, count))
+    ws = torch.empty(hsi.detect_batch_workspace_bytes(jobs), dtype=torch.uint8, device="cuda")
+    hsi.detect_batch(jobs, ws)
+    torch.cuda.synchronize()
+    for score, target, H, W, thr, r, higher, _, _, out, count in keep:
+        n0, want = orc.detect(score, target, H, W, thr, r, higher, capacity=H * W + 1)
+        n, got = hsi.detections_to_numpy(count, out, H * W + 1)
+        assert n == n0
+        assert _tuples(got) == _tuples(want)
