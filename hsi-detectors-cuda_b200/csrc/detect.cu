@@ -15,6 +15,8 @@
 // Semantics are the reference CPU path's (src/sam_cpu.cpp:86-138), polarity
 // included; the reference GPU kernel (src/detect.cu:43-87) ignores polarity
 // and emits in atomic arrival order, both of which this replaces.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace hsi_b200 {
@@ -351,4 +353,80 @@ extern "C" HSI_API int hsi_detect(const float* d_score, const int32_t* d_target,
 extern "C" HSI_API int hsi_detect_batch(const hsi_detect_job* jobs, int num_jobs, void* d_workspace,
                                         size_t workspace_bytes, hsi_stream_t stream) {
   return run_batch(jobs, num_jobs, d_workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
+// ---- allocation-free detection ------------------------------------------------
+//
+// For callers that cannot allocate device memory at all -- for example a
+// plug-in that a host application hands only its input and output buffers,
+// while the application owns every byte of device memory and lets nothing
+// else call cudaMalloc -- hsi_detect_noalloc runs the same three launches as
+// hsi_detect with its scratch in the file-scope array below instead of a
+// caller workspace.  The array is part of the library's device image, so
+// every GPU that loads the library holds it (2.06 MiB) until the process
+// exits, and every call on one device shares it.
+namespace hsi_b200 {
+namespace {
+
+constexpr int kNoAllocSegs = HSI_DETECT_NOALLOC_MAX_SEGMENTS;
+constexpr size_t kNoAllocBytes = static_cast<size_t>(kNoAllocSegs) * sizeof(uint32_t) * (2 + kWordsPerSeg) + 256;
+
+// Segment counts, offsets and ballot masks of one call.  Every word a call
+// reads is written earlier by that same call (flags writes counts and all 64
+// mask words of each segment, scan writes offsets), so nothing here needs to
+// start at zero and stale contents from a previous call are never read.
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocBytes / sizeof(uint32_t)];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[kNoAllocMaxDevices];  // device address of the array, per device
+
+// Once per device, with that device current: look up the array's device
+// address (in host code its name is only a host-side stand-in) and allow the
+// flags kernel its full shared-memory tile on this device.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return static_cast<int>(e);
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return HSI_E_NO_DEVICE;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_addr[dev] == nullptr) {
+    void* addr = nullptr;
+    e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess) return static_cast<int>(e);
+    if ((reinterpret_cast<uintptr_t>(addr) & 255u) != 0) return HSI_E_INVALID;
+    e = cudaFuncSetAttribute(flags_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>((2 * kMaxStagedRadius + 1) * (kSeg + 2 * kMaxStagedRadius) *
+                                              sizeof(float)));
+    if (e != cudaSuccess) return static_cast<int>(e);
+    g_noalloc_addr[dev] = addr;
+  }
+  *out = g_noalloc_addr[dev];
+  return HSI_OK;
+}
+
+}  // namespace
+}  // namespace hsi_b200
+
+extern "C" HSI_API int hsi_detect_noalloc(const float* d_score, const int32_t* d_target, int height, int width,
+                                          float threshold, int nms_radius, int polarity, int capacity,
+                                          hsi_detection* d_out, uint32_t* d_count, hsi_stream_t stream) {
+  if (height <= 0 || width <= 0) return HSI_E_INVALID;
+  const int64_t segs = static_cast<int64_t>(height) * ((static_cast<int64_t>(width) + kSeg - 1) / kSeg);
+  if (segs > kNoAllocSegs) return HSI_E_CAPACITY;
+  void* scratch = nullptr;
+  const int st = noalloc_scratch(&scratch);
+  if (st != HSI_OK) return st;
+  hsi_detect_job j;
+  j.score = d_score;
+  j.target = d_target;
+  j.height = height;
+  j.width = width;
+  j.threshold = threshold;
+  j.nms_radius = nms_radius;
+  j.polarity = polarity;
+  j.capacity = capacity;
+  j.out = d_out;
+  j.count = d_count;
+  return run_batch(&j, 1, scratch, kNoAllocBytes, reinterpret_cast<cudaStream_t>(stream));
 }

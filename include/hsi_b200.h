@@ -287,6 +287,32 @@ HSI_API size_t hsi_detect_batch_workspace_bytes(const hsi_detect_job* jobs, int 
 HSI_API int hsi_detect_batch(const hsi_detect_job* jobs, int num_jobs, void* d_workspace,
                              size_t workspace_bytes, hsi_stream_t stream);
 
+/* Allocation-free detection.  No counterpart in the reference: it is for
+ * callers that cannot allocate device memory at all (for example a plug-in
+ * that its host application hands only input and output buffers, the
+ * application owning all device memory), so they cannot provide the
+ * workspace hsi_detect needs.  Same arguments, semantics and results as
+ * hsi_detect, without the workspace: the scratch is a 2.06 MiB array inside
+ * the library's device image, which every GPU that loads the library holds
+ * until the process exits.  Limits and rules:
+ *  - height * ceil(width / 2048) must not exceed
+ *    HSI_DETECT_NOALLOC_MAX_SEGMENTS (e.g. 8192 rows of up to 2048 pixels,
+ *    or 4096 x 4096); larger maps return HSI_E_CAPACITY;
+ *  - every call on a device shares that one array, so calls whose work
+ *    overlaps on the GPU (on different streams, or from different host
+ *    threads without ordering) race and corrupt each other's lists; calls on
+ *    one stream are ordered and safe;
+ *  - the scratch needs no clearing; as with hsi_detect, *d_count is the
+ *    append offset the caller sets (normally zero) before the call;
+ *  - the first call on each device does a one-time set-up (it looks up the
+ *    array's device address and sets the detection kernel's shared-memory
+ *    limit), so that first call should come before any stream capture.
+ * It calls no allocating routine.  HSI_E_NO_DEVICE for device ordinals >= 64. */
+#define HSI_DETECT_NOALLOC_MAX_SEGMENTS 8192
+HSI_API int hsi_detect_noalloc(const float* d_score, const int32_t* d_target, int height, int width,
+                               float threshold, int nms_radius, int polarity, int capacity,
+                               hsi_detection* d_out, uint32_t* d_count, hsi_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
