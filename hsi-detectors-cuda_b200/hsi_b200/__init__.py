@@ -136,7 +136,10 @@ def _optional_symbols(L):
         "hsi_rx_ace": ([vp, i32, i32, i32, i32, i64, vp, i32, vp, vp, vp, vp, i64, vp, C.c_size_t, vp], i32),
         "hsi_rx_ace_simt_workspace_bytes": ([i32, i32], C.c_size_t),
         "hsi_rx_ace_simt": ([vp, i32, i32, i32, i32, i64, vp, i32, vp, vp, vp, vp, i64, vp, C.c_size_t, vp], i32),
-        "hsi_demosaic": ([vp, i32, i32, i32, i32, vp, vp, i64, vp], i32),
+        "hsi_demosaic": ([vp, i32, i32, i32, i32, vp, vp, i32, i64, vp], i32),
+        "hsi_narrow_to_half": ([vp, vp, i64, vp], i32),
+        "hsi_transpose_bip_to_bsq": ([vp, vp, i32, i32, i32, i64, vp], i32),
+        "hsi_accumulate_shifted_moments": ([vp, vp, i32, vp, vp, vp], i32),
         "hsi_detect_noalloc": ([vp, vp, i32, i32, C.c_float, i32, i32, i32, vp, vp, vp], i32),
     }
     for name, (argtypes, restype) in table.items():

@@ -287,6 +287,39 @@ HSI_API size_t hsi_detect_batch_workspace_bytes(const hsi_detect_job* jobs, int 
 HSI_API int hsi_detect_batch(const hsi_detect_job* jobs, int num_jobs, void* d_workspace,
                              size_t workspace_bytes, hsi_stream_t stream);
 
+/* ---- data formats ------------------------------------------------------------ */
+
+/* fp32 -> fp16 (round to nearest even) of `count` elements; d_src 16-byte and
+ * d_dst 8-byte aligned.  Replaces hsi::launch_narrow_to_half (reference
+ * include/hsi/sam_cuda.hpp:108-109, src/sam.cu:311-316,476-482). */
+HSI_API int hsi_narrow_to_half(const float* d_src, void* d_dst, int64_t count, hsi_stream_t stream);
+
+/* BIP (pixel-major, `bands` floats per pixel) -> BSQ planes at `plane_stride`.
+ * Replaces hsi::launch_transpose_bip_to_bsq (reference
+ * include/hsi/sam_cuda.hpp:104-105, src/sam.cu:281-309,463-474), which writes
+ * packed planes. */
+HSI_API int hsi_transpose_bip_to_bsq(const float* d_src, float* d_dst, int height, int width, int bands,
+                                     int64_t plane_stride, hsi_stream_t stream);
+
+/* Snapshot-mosaic demosaic on the device: raw frame (raw_height x raw_width
+ * floats, row-major) -> BSQ cube of (raw_height/period) x (raw_width/period)
+ * pixels and `bands` <= period^2 bands, element type `dtype`.  Band b takes
+ * the mosaic position band_order[b] (HOST array, nullable: position b);
+ * positions outside [0, period^2) return HSI_E_INVALID.  Same mapping as the
+ * reference's demosaic (src/hot_loader.cpp:144-182). */
+HSI_API int hsi_demosaic(const float* d_raw, int raw_height, int raw_width, int period, int bands,
+                         const int32_t* band_order, void* d_cube, int dtype, int64_t plane_stride,
+                         hsi_stream_t stream);
+
+/* Add the sums about a reference spectrum, S1 = sum(x - r) and the lower
+ * triangle (row-major, B*B buffer) of S2 = sum (x - r)(x - r)^T, of raw FP64
+ * moments (hsi_scene_moments output) into the caller's accumulators.
+ * `d_reference` nullable (r = 0).  Gives hsi_scene_moments the accumulate
+ * contract of the reference's launch_accumulate_moments
+ * (include/hsi/stats_cuda.hpp:52-55, src/stats.cu:169-248). */
+HSI_API int hsi_accumulate_shifted_moments(const double* d_moments, const float* d_reference, int bands,
+                                           double* d_sum, double* d_sum_outer, hsi_stream_t stream);
+
 /* Allocation-free detection.  No counterpart in the reference: it is for
  * callers that cannot allocate device memory at all (for example a plug-in
  * that its host application hands only input and output buffers, the
