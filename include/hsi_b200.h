@@ -237,6 +237,18 @@ HSI_API int hsi_build_statistics(int num_frames, int bands, int num_targets, dou
  * (P int32), `d_ace_maps` (num_targets maps at `map_stride`).  At most 16
  * targets per call.
  */
+/* Tensor-core path: the augmented whitener [W; (W^T u_t)^T] and the centred
+ * pixels in exact fixed point (per-row and per-pixel power-of-two scales,
+ * signed 8-bit limbs, tcgen05 INT8 MMAs into INT32), combined in FP32; error
+ * against FP64 a few 1e-5 (RX relative to max(1, RX), ACE absolute) at 113
+ * bands.  bands <= 127 (else HSI_E_CAPACITY); targets beyond 128 - bands per
+ * pass take further passes over the cube, the best carried in the outputs.
+ * Workspace: hsi_rx_ace_workspace_bytes (256-byte aligned). */
+HSI_API size_t hsi_rx_ace_workspace_bytes(int bands, int num_targets);
+HSI_API int hsi_rx_ace(const void* d_cube, int height, int width, int bands, int dtype, int64_t plane_stride,
+                       const double* d_stats64, int num_targets, float* d_rx, float* d_ace_best,
+                       int32_t* d_ace_target, float* d_ace_maps, int64_t map_stride, void* d_workspace,
+                       size_t workspace_bytes, hsi_stream_t stream);
 HSI_API size_t hsi_rx_ace_simt_workspace_bytes(int bands, int num_targets);
 /* Plain FP32 CUDA-core path (register-blocked GEMM over [W; (W^T U)^T]). */
 HSI_API int hsi_rx_ace_simt(const void* d_cube, int height, int width, int bands, int dtype,

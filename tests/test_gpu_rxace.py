@@ -51,9 +51,13 @@ def _check_scores(orc, host, S, rx, ace, at, maps, T):
     return rx_err
 
 
-@pytest.mark.parametrize("simt", [True])
-@pytest.mark.parametrize("B,T", [(16, 3), (113, 8), (127, 1), (224, 16)])
+@pytest.mark.parametrize("simt", [True, False])
+@pytest.mark.parametrize("B,T", [(16, 3), (113, 8), (127, 1), (113, 16), (224, 16)])
 def test_rx_ace_with_fp64_statistics(hsi, orc, simt, B, T):
+    """simt=False is the tensor-core path (INT8 limbs); (113, 16) takes two
+    target passes there (15 + 1 targets), the best carried between them."""
+    if not simt and B > 127:
+        pytest.skip("the tensor-core path holds at most 127 bands")
     H, W = 96, 80
     cube, _, lib = _scene(hsi, H, W, B, T, seed=B * 7 + T)
     P = H * W
@@ -69,7 +73,34 @@ def test_rx_ace_with_fp64_statistics(hsi, orc, simt, B, T):
     _check_scores(orc, host, S, rx.cpu().numpy(), ace.cpu().numpy(), at.cpu().numpy(), maps.cpu().numpy(), T)
 
 
-def test_rx_ace_reference_properties(hsi, orc):
+@pytest.mark.parametrize("dtype", [0, 1])
+def test_rx_ace_tensor_core_at_size(hsi, orc, dtype):
+    """512 x 512 x 113 with anomalies, 8 targets, both cube types: the tensor-core
+    path against the FP64 oracle on the same (device-read-back) cube."""
+    H, W, B, T = 512, 512, 113, 8
+    cube, _, lib = _scene(hsi, H, W, B, T, seed=0x5EED2001, dtype=dtype)
+    P = H * W
+    host = _download(cube, B, P)
+    S = _fp64_stats(orc, host, lib, 1e-6)
+    stats = torch.from_numpy(_pack(S)).cuda()
+    rx = torch.zeros(P, device="cuda")
+    ace = torch.zeros(P, device="cuda")
+    at = torch.zeros(P, dtype=torch.int32, device="cuda")
+    maps = torch.zeros((T, P), device="cuda")
+    hsi.rx_ace(cube, H, W, B, stats, T, dtype=dtype, rx=rx, ace_best=ace, ace_target=at, ace_maps=maps, simt=False)
+    torch.cuda.synchronize()
+    _check_scores(orc, host, S, rx.cpu().numpy(), ace.cpu().numpy(), at.cpu().numpy(), maps.cpu().numpy(), T)
+
+
+def test_rx_ace_tensor_core_rejects_too_many_bands(hsi):
+    cube = torch.zeros((128, 64), device="cuda")
+    stats = torch.zeros(128 + 128 * 128, dtype=torch.float64, device="cuda")
+    with pytest.raises(hsi.HsiError):
+        hsi.rx_ace(cube, 8, 8, 128, stats, 0, rx=torch.zeros(64, device="cuda"), simt=False)
+
+
+@pytest.mark.parametrize("simt", [True, False])
+def test_rx_ace_reference_properties(hsi, orc, simt):
     """RX ranks planted anomalies above the background, ACE peaks on its own
     target (tests/test_detectors.cpp:82-184), on the GPU path."""
     H, W, B = 40, 48, 14
@@ -93,7 +124,7 @@ def test_rx_ace_reference_properties(hsi, orc):
     rx = torch.zeros(P, device="cuda")
     ace = torch.zeros(P, device="cuda")
     at = torch.zeros(P, dtype=torch.int32, device="cuda")
-    hsi.rx_ace(cube, H, W, B, s64[0], 2, rx=rx, ace_best=ace, ace_target=at, simt=True)
+    hsi.rx_ace(cube, H, W, B, s64[0], 2, rx=rx, ace_best=ace, ace_target=at, simt=simt)
     torch.cuda.synchronize()
     assert int(status[0]) == 0
     rx, ace, at = rx.cpu().numpy(), ace.cpu().numpy(), at.cpu().numpy()
