@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default=None, choices=["sam", "sam_cem"])
+    ap.add_argument("--workload", default=None, choices=["sam", "sam_cem", "rx_ace"])
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -76,15 +76,17 @@ def cpu_reference(workload, sample_rows, repeats, threads=None):
     import oracle
     lib = oracle.ref_lib()
     threads = threads or len(os.sched_getaffinity(0))
-    spec = oracle.scene(B, n_targets=TARGETS, target_frac=0.002, library_seed=0x5EED1000)
+    seed = 0x5EED2000 if workload == "rx_ace" else 0x5EED1000
+    anomaly = 0.001 if workload == "rx_ace" else 0.0
+    spec = oracle.scene(B, n_targets=TARGETS, target_frac=0.002, library_seed=seed)
     _, targets, _ = oracle.scene_spectra(spec.library_seed, B, 6, TARGETS)
     targets = np.ascontiguousarray(targets)
     norms = oracle.ref_norms(targets)
     P = W * sample_rows
     cubes = []
     for t in range(threads):
-        s = oracle.scene(B, n_targets=TARGETS, target_frac=0.002, library_seed=0x5EED1000,
-                         frame_seed=0x5EED1000 + t)
+        s = oracle.scene(B, n_targets=TARGETS, target_frac=0.002, anomaly_frac=anomaly, library_seed=seed,
+                         frame_seed=seed + 1 + t)
         cubes.append(oracle.generate(s, sample_rows, W)[0])
     f32, i32 = C.POINTER(C.c_float), C.POINTER(C.c_int32)
 
@@ -96,7 +98,10 @@ def cpu_reference(workload, sample_rows, repeats, threads=None):
         ct = np.empty(P, np.int32)
         dets = np.zeros(CAPACITY, oracle.DETECTION_DTYPE)
         cp = cube.ctypes.data_as(f32)
-        if workload == "sam_cem":
+        if workload == "rx_ace":
+            lib.ref_frame_rx_ace(cp, sample_rows, W, B, targets.ctypes.data_as(f32), TARGETS, LOADING,
+                                 cem.ctypes.data_as(f32), ct.ctypes.data_as(i32), best.ctypes.data_as(f32))
+        elif workload == "sam_cem":
             lib.ref_frame_sam_cem(cp, sample_rows, W, B, targets.ctypes.data_as(f32), TARGETS, LOADING,
                                   THRESHOLD, NMS_RADIUS, maps.ctypes.data_as(f32), best.ctypes.data_as(f32),
                                   bt.ctypes.data_as(i32), cem.ctypes.data_as(f32), ct.ctypes.data_as(i32),
@@ -144,10 +149,17 @@ def run_reference(args, workload):
 
 
 def metric_name(workload):
+    if workload == "rx_ace":
+        return "Mpix/s RX+ACE @113 bands"
     return "Mpix/s SAM+CEM @113 bands" if workload == "sam_cem" else "Mpix/s SAM @113 bands"
 
 
 def workload_config(workload, frames, reference=False):
+    if workload == "rx_ace":
+        return {"workload": f"one {RX_H}x{RX_W}x{B} f32 frame per GPU, {TARGETS} ACE targets: scene moments + "
+                            "FP64 factor + whitening (RX + ACE maps + best)",
+                "height": RX_H, "width": RX_W, "bands": B, "targets": TARGETS, "diagonal_loading": LOADING,
+                "l2": "host CPU" if reference else "inputs larger than L2 (947.9 MB cube)"}
     cfg = {
         "workload": (f"{frames} frames {H}x{W}x{B} f32, {TARGETS} targets: "
                      + ("scene correlation + FP64 factor + fused SAM/CEM maps" if workload == "sam_cem"
@@ -527,6 +539,195 @@ def run_e2e(hsi, torch, wl, stream, args, world):
             "ms_per_step": round(ms, 3), "path": "C ABI (hsi_score_frames + hsi_detect) from pinned host cubes"}
 
 
+# ---------------------------------------------------------------------------
+# RX + ACE precision workload: one 2048 x 1024 x 113 frame, 8 ACE targets
+# ---------------------------------------------------------------------------
+
+RX_H, RX_W = 2048, 1024
+
+
+def _fp64_reference(torch, cube, H, Wd, lib, rows):
+    """Plain torch FP64 RX/ACE on the first `rows` rows, from FP64 statistics of
+    the whole frame (the error reference; not the measured path)."""
+    P = H * Wd
+    x = cube[:, :P].double()
+    mu = x.mean(dim=1)
+    xc = x - mu[:, None]
+    S = (xc @ xc.T) / P + LOADING * torch.eye(B, dtype=torch.float64, device=cube.device)
+    Lc = torch.linalg.cholesky(S)
+    Wm = torch.linalg.solve_triangular(Lc, torch.eye(B, dtype=torch.float64, device=cube.device), upper=False)
+    U = Wm @ (lib.double() - mu[None, :]).T          # B x T
+    uu = (U * U).sum(dim=0)
+    z = Wm @ xc[:, :rows * Wd]
+    rx = (z * z).sum(dim=0)
+    maps = (U.T @ z) ** 2 / (uu[:, None] * rx[None, :])
+    return rx, maps
+
+
+def run_rxace(args):
+    import ctypes as C
+    import torch
+    import hsi_b200 as hsi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    device = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(device)
+    L = hsi.lib()
+    H, Wd, T = RX_H, RX_W, TARGETS
+    P = H * Wd
+    sc = hsi.scene(B, n_targets=T, target_frac=0.002, anomaly_frac=0.001, library_seed=0x5EED2000,
+                   frame_seed=0x5EED2001 + rank)
+    cube, _ = hsi.generate(sc, H, Wd, truth=False, device=device)
+    stride = hsi.plane_stride(H, Wd)
+    lib = torch.from_numpy(hsi.scene_targets(sc)).to(device)
+    moments = torch.zeros(B + B * B + 1, dtype=torch.float64, device=device)
+    stats64 = torch.zeros(L.hsi_statistics_elements(B, T), dtype=torch.float64, device=device)
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    sws_b = L.hsi_stats_workspace_bytes(H, Wd, B)
+    sws = torch.empty(sws_b, dtype=torch.uint8, device=device)
+    rx = torch.empty(P, device=device)
+    ab = torch.empty(P, device=device)
+    at = torch.empty(P, dtype=torch.int32, device=device)
+    maps = torch.empty((T, P), device=device)
+    tws_b = L.hsi_rx_ace_workspace_bytes(B, T)
+    tws = torch.empty(tws_b, dtype=torch.uint8, device=device)
+    pws_b = L.hsi_rx_ace_simt_workspace_bytes(B, T)
+    pws = torch.empty(pws_b, dtype=torch.uint8, device=device)
+    stream = torch.cuda.current_stream(device)
+    s = C.c_void_p(stream.cuda_stream)
+    vp = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+
+    def statistics(src):
+        hsi.check(L.hsi_scene_moments(vp(src), H, Wd, B, 0, stride, vp(moments), None, vp(sws), sws_b, s), "moments")
+        hsi.check(L.hsi_build_statistics(1, B, T, LOADING, vp(moments), vp(lib), 0, vp(stats64), None, None,
+                                         vp(status), None, 0, s), "statistics")
+
+    def score(src, plain):
+        fn = L.hsi_rx_ace_simt if plain else L.hsi_rx_ace
+        ws, wb = (pws, pws_b) if plain else (tws, tws_b)
+        hsi.check(fn(vp(src), H, Wd, B, 0, stride, vp(stats64), T, vp(rx), vp(ab), vp(at), vp(maps), P, vp(ws), wb,
+                     s), "rx_ace")
+
+    def timed(plain, steps, warmup):
+        ev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(steps)]
+        for _ in range(warmup):
+            statistics(cube)
+            score(cube, plain)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(steps):
+            ev[k][0].record(stream)
+            statistics(cube)
+            ev[k][1].record(stream)
+            score(cube, plain)
+            ev[k][2].record(stream)
+        torch.cuda.synchronize()
+        step = float(np.mean([a.elapsed_time(c) for a, _, c in ev]))
+        kern = float(np.mean([b.elapsed_time(c) for _, b, c in ev]))
+        return step, kern
+
+    props = torch.cuda.get_device_properties(device)
+    uuid = getattr(props, "uuid", None)
+    uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else (str(uuid) if uuid else None)
+    with ClockSampler(uuid) as clocks:
+        ms, kern_ms = timed(False, args.steps, args.warmup)
+    plain_ms, plain_kern = timed(True, max(2, args.steps // 2), 1)
+    if dist:
+        t = torch.tensor([ms, kern_ms, plain_ms, plain_kern], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, kern_ms, plain_ms, plain_kern = [float(v) for v in t]
+
+    # error of the measured path against a torch FP64 reference (first 64 rows)
+    statistics(cube)
+    score(cube, False)
+    torch.cuda.synchronize()
+    rows = 64
+    rx64, maps64 = _fp64_reference(torch, cube, H, Wd, lib, rows)
+    n = rows * Wd
+    rx_err = ((rx[:n].double() - rx64).abs() / rx64.abs().clamp(min=1.0))
+    map_err = (maps[:, :n].double() - maps64).abs()
+    best64 = maps64.clamp(0, 1).max(dim=0).values
+    ace_err = (ab[:n].double() - best64).abs()
+    errors = {"reference": "torch FP64 statistics of the whole frame + FP64 scores, first 64 rows (65536 px)",
+              "rx_rel": {"max": float(rx_err.max()), "mean": float(rx_err.mean())},
+              "ace_best_abs": {"max": float(ace_err.max()), "mean": float(ace_err.mean())},
+              "ace_maps_abs": {"max": [float(v) for v in map_err.max(dim=1).values],
+                               "mean": [float(v) for v in map_err.mean(dim=1)]}}
+
+    e2e = None
+    dev = None
+    if not args.no_e2e:
+        host = torch.empty_like(cube, device="cpu").pin_memory()
+        host.copy_(cube)
+        dev = torch.empty_like(cube)
+        out_host = torch.empty((2, P), dtype=torch.float32).pin_memory()
+
+        def e2e_step():
+            dev.copy_(host, non_blocking=True)
+            statistics(dev)
+            score(dev, False)
+            out_host[0].copy_(rx, non_blocking=True)
+            out_host[1].copy_(ab, non_blocking=True)
+        e2e_step()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        e_ms = a.elapsed_time(b) / args.steps
+        e2e = {"value": round(world * P / (e_ms / 1e3) / 1e6, 2), "unit": "Mpix/s",
+               "h2d_bytes_per_step": host.numel() * host.element_size(), "d2h_bytes_per_step": out_host.numel() * 4,
+               "ms_per_step": round(e_ms, 3), "path": "C ABI (hsi_scene_moments + hsi_build_statistics + hsi_rx_ace)"}
+
+    del cube, dev
+    torch.cuda.empty_cache()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        times, threads, Ps = cpu_reference("rx_ace", 128, 2)
+        t = float(np.mean(times))
+        cpu = {"value": round(threads * Ps / t / 1e6, 3), "unit": "Mpix/s", "cores": threads, "kind": "reference",
+               "sample": f"{threads} frames of {W}x128x{B}, one per thread (moments + statistics + ace_best_cpu "
+                         "with RX), mean of 2 runs"}
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    per_px = 4 * B + 4 + 4 * T + 8  # cube + RX + ACE maps + best score / id
+    ach = P * per_px / (kern_ms / 1e3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": metric_name("rx_ace"), "value": round(world * P / (ms / 1e3) / 1e6, 2), "unit": "Mpix/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8-limb/f32",
+            "data": "synthetic (seeded scene model generated on the device, 0.1% anomalies)",
+            "config": dict(workload_config("rx_ace", 1), parallelism=f"one frame per GPU over {world} GPU(s)"),
+            "roofline": {"kernel": "rxace_tc_kernel (+ its prep)", "bound": "hbm", "achieved": round(ach, 1),
+                         "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": None,
+                         "kernel_ms": round(kern_ms, 3), "algorithmic_bytes_per_launch": P * per_px},
+            "plain_fp32": {"step_ms": round(plain_ms, 3), "kernel_ms": round(plain_kern, 3),
+                           "kernel_mpix_s": round(P / (plain_kern / 1e3) / 1e6, 1),
+                           "tensor_core_speedup": round(plain_kern / kern_ms, 2)},
+            "errors_vs_fp64": errors,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 6 + 1 + 2, "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -537,6 +738,9 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": f"{type(e).__name__}: {e}"}), flush=True)
         return
     workload = args.workload or DEFAULT_WORKLOAD
+    if workload == "rx_ace":
+        run_rxace(args)
+        return
     run_ours(args, workload)
 
 

@@ -144,19 +144,6 @@ struct StatsArgs {
   int* status;
 };
 
-// Split q (|q| <= kQMax) into balanced signed bytes: q = l0*2^16 + l1*2^8 + l2.
-__device__ __forceinline__ void limbs(int q, int& l0, int& l1, int& l2) {
-  l2 = ((q + 128) & 255) - 128;
-  const int q1 = (q - l2) >> 8;
-  l1 = ((q1 + 128) & 255) - 128;
-  l0 = (q1 - l1) >> 8;
-}
-
-__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
-  return (static_cast<uint32_t>(a) & 255u) | ((static_cast<uint32_t>(b) & 255u) << 8) |
-         ((static_cast<uint32_t>(c) & 255u) << 16) | ((static_cast<uint32_t>(d) & 255u) << 24);
-}
-
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 1)
     stats_gemm_kernel(const __grid_constant__ CUtensorMap cube_map, const StatsArgs args) {
