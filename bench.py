@@ -407,7 +407,7 @@ def run_ours(args, workload):
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = algorithmic_bytes_score(args.frames, wl.cem) / (kernel_ms / 1e3) / 1e9
-    traffic = load_traffic(workload)
+    traffic = load_traffic(workload, args.frames)
     roofline = {"kernel": "score_kernel (fused SAM/CEM filter bank)", "bound": "hbm",
                 "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
@@ -453,14 +453,17 @@ def run_ours(args, workload):
         dist.destroy_process_group()
 
 
-def load_traffic(workload):
-    """DRAM bytes per launch of the scoring kernel from the committed ncu summary, if present."""
-    path = os.path.join(REPO, "profiles", "traffic.json")
-    try:
-        d = json.load(open(path))
-        return d.get(workload)
-    except Exception:
-        return None
+# DRAM bytes (read + write) per frame of the scoring kernel, from the ncu
+# captures summarised in profiles/ (score_kernel_samcem8_f32_1024x1024x113.md:
+# 2.219 GB for a 4-frame launch; rxace_tc_kernel_f32_2048x1024x113.md: one
+# frame).  The scorer's traffic grows with the frames in the launch.
+TRAFFIC_PER_FRAME = {"sam_cem": 554.63e6, "rx_ace": 1036.90e6}
+
+
+def load_traffic(workload, frames):
+    """DRAM bytes per launch of the dominant kernel, scaled from the capture."""
+    per = TRAFFIC_PER_FRAME.get(workload)
+    return None if per is None else round(per * frames)
 
 
 def run_e2e(hsi, torch, wl, stream, args, world):
@@ -715,7 +718,8 @@ def run_rxace(args):
             "data": "synthetic (seeded scene model generated on the device, 0.1% anomalies)",
             "config": dict(workload_config("rx_ace", 1), parallelism=f"one frame per GPU over {world} GPU(s)"),
             "roofline": {"kernel": "rxace_tc_kernel (+ its prep)", "bound": "hbm", "achieved": round(ach, 1),
-                         "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": None,
+                         "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
+                         "traffic": load_traffic("rx_ace", 1),
                          "kernel_ms": round(kern_ms, 3), "algorithmic_bytes_per_launch": P * per_px},
             "plain_fp32": {"step_ms": round(plain_ms, 3), "kernel_ms": round(plain_kern, 3),
                            "kernel_mpix_s": round(P / (plain_kern / 1e3) / 1e6, 1),
