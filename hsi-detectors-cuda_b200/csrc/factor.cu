@@ -13,7 +13,10 @@
 // All arithmetic is FP64, because the factorisation of a nearly rank-6
 // covariance needs it.  One CTA per frame; frames of a batch factor in
 // parallel.  Matrices live in shared memory as packed lower triangles when
-// they fit (B <= 128) and in the caller's workspace otherwise.
+// they fit (B <= 128) and in the caller's workspace otherwise.  The solves use
+// the explicit triangular inverses (blocked, parallel) rather than sequential
+// substitution, so a single frame factors in ~0.1 ms instead of being bound by
+// ~10^4 dependent FP64 steps.
 #include "common.cuh"
 
 namespace hsi_b200 {
@@ -22,9 +25,11 @@ namespace {
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSmemMaxBands = 128;
+constexpr int kChunk = 16;  // targets per pass through the per-target buffers
+constexpr int kBlk = 16;    // row block of the triangular inverse
 
 __host__ __device__ inline size_t tri(int n) { return static_cast<size_t>(n) * (n + 1) / 2; }
-__device__ __forceinline__ size_t pk(int i, int j) { return static_cast<size_t>(i) * (i + 1) / 2 + j; }  // j <= i
+__device__ __forceinline__ size_t row_off(int i) { return static_cast<size_t>(i) * (i + 1) / 2; }
 
 struct FactorArgs {
   int bands, targets;
@@ -46,40 +51,111 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// In-place right-looking Cholesky of a packed lower triangle.  Returns false
-// (to every thread) if a pivot is not positive or is NaN (src/linalg.cpp:105-122).
-__device__ bool cholesky_packed(double* a, int n, int* s_flag) {
-  for (int k = 0; k < n; ++k) {
-    if (threadIdx.x == 0) {
-      const double d = a[pk(k, k)];
-      if (!(d > 0.0)) *s_flag = 1;
-      else a[pk(k, k)] = sqrt(d);
+// Fill the packed lower triangle with M2/N (- mean mean^T) + loading I.
+__device__ void fill_matrix(double* A, const double* outer, const double* mean, double N, double loading, int n,
+                            bool centred) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = warp; i < n; i += kWarps) {
+    double* ri = A + row_off(i);
+    for (int j = lane; j <= i; j += 32) {
+      double v = outer[static_cast<size_t>(i) * n + j] / N;
+      if (centred) v -= mean[i] * mean[j];
+      if (i == j) v += loading;
+      ri[j] = v;
     }
-    __syncthreads();
-    if (*s_flag) return false;
-    const double piv = a[pk(k, k)];
-    for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) a[pk(i, k)] /= piv;
-    __syncthreads();
-    // trailing update of rows i > k, columns k < j <= i
-    const int m = n - k - 1;
-    const size_t work = tri(m);
-    for (size_t e = threadIdx.x; e < work; e += blockDim.x) {
-      // decode e -> (ii, jj) with jj <= ii < m
-      int ii = static_cast<int>((sqrt(8.0 * static_cast<double>(e) + 1.0) - 1.0) * 0.5);
-      while (tri(ii + 1) <= e) ++ii;
-      while (tri(ii) > e) --ii;
-      const int jj = static_cast<int>(e - tri(ii));
-      const int i = k + 1 + ii, j = k + 1 + jj;
-      a[pk(i, j)] -= a[pk(i, k)] * a[pk(j, k)];
+  }
+  __syncthreads();
+}
+
+// In-place right-looking Cholesky of a packed lower triangle, one barrier per
+// elimination step: step k subtracts a_ik a_jk / a_kk from the trailing
+// triangle with the column left unscaled, and all columns are scaled by
+// 1/sqrt(pivot) at the end.  Returns false -- the same on every thread, which
+// all read the same pivot -- if a pivot is not positive or is NaN
+// (src/linalg.cpp:105-122).  `dv`: n doubles of scratch.
+__device__ bool cholesky_packed(double* a, int n, double* dv) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int k = 0; k < n; ++k) {
+    const double d = a[row_off(k) + k];
+    if (!(d > 0.0)) return false;
+    const double inv = 1.0 / d;
+    for (int i = k + 1 + warp; i < n; i += kWarps) {
+      double* ri = a + row_off(i);
+      const double f = ri[k] * inv;
+      for (int j = k + 1 + lane; j <= i; j += 32) ri[j] -= f * a[row_off(j) + k];
     }
     __syncthreads();
   }
+  for (int k = threadIdx.x; k < n; k += blockDim.x) dv[k] = sqrt(a[row_off(k) + k]);
+  __syncthreads();
+  for (int i = warp; i < n; i += kWarps) {
+    double* ri = a + row_off(i);
+    for (int j = lane; j <= i; j += 32) ri[j] = j == i ? dv[i] : ri[j] / dv[j];
+  }
+  __syncthreads();
   return true;
+}
+
+// Winv = L^-1 (both packed lower) by blocked forward substitution on L X = I
+// (src/linalg.cpp:150-162 solves the same system column by column).  Per row
+// block [r0, r1): first every (row, column) takes the part of its sum over the
+// finished rows j < r0 in parallel, then each thread finishes one column down
+// the block's rows.
+__device__ void triangular_inverse(const double* L, double* Winv, int n) {
+  for (int r0 = 0; r0 < n; r0 += kBlk) {
+    const int r1 = min(r0 + kBlk, n);
+    const int work = (r1 - r0) * r1;
+    for (int e = threadIdx.x; e < work; e += blockDim.x) {
+      const int i = r0 + e / r1, c = e % r1;
+      if (c > i) continue;
+      double s = c == i ? 1.0 : 0.0;
+      if (c < r0) {
+        const double* li = L + row_off(i);
+        for (int j = c; j < r0; ++j) s -= li[j] * Winv[row_off(j) + c];
+      }
+      Winv[row_off(i) + c] = s;
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < r1; c += blockDim.x) {
+      const int j0 = max(r0, c);
+      for (int i = j0; i < r1; ++i) {
+        const double* li = L + row_off(i);
+        double s = Winv[row_off(i) + c];
+        for (int j = j0; j < i; ++j) s -= li[j] * Winv[row_off(j) + c];
+        Winv[row_off(i) + c] = s / li[i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// out[t][i] = sum_{j <= i} M[i][j] v[t][j] (M packed lower), t < nt.
+__device__ void lower_matvec(const double* M, const double* v, double* out, int n, int nt) {
+  for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
+    const int t = e / n, i = e % n;
+    const double* mi = M + row_off(i);
+    const double* vt = v + static_cast<size_t>(t) * n;
+    double s = 0.0;
+    for (int j = 0; j <= i; ++j) s += mi[j] * vt[j];
+    out[e] = s;
+  }
+  __syncthreads();
+}
+
+// out[t][i] = sum_{k >= i} M[k][i] v[t][k] (M^T, M packed lower), t < nt.
+__device__ void upper_matvec(const double* M, const double* v, double* out, int n, int nt) {
+  for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
+    const int t = e / n, i = e % n;
+    const double* vt = v + static_cast<size_t>(t) * n;
+    double s = 0.0;
+    for (int k = i; k < n; ++k) s += M[row_off(k) + i] * vt[k];
+    out[e] = s;
+  }
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(kThreads) factor_kernel(const FactorArgs args) {
   extern __shared__ double smem[];
-  __shared__ int s_flag;
   const int f = blockIdx.x;
   const int B = args.bands, T = args.targets;
   const double* mom = args.moments + f * args.moments_stride;
@@ -89,15 +165,15 @@ __global__ void __launch_bounds__(kThreads) factor_kernel(const FactorArgs args)
   float* out32 = args.stats32 ? args.stats32 + f * per : nullptr;
   float* cem32 = args.cem32 ? args.cem32 + static_cast<size_t>(f) * T * B : nullptr;
   const bool in_smem = B <= kSmemMaxBands;
-  // smem: mean[B], T x B target work vectors, one solve vector per warp,
-  // then the packed matrices (in the workspace when B is large)
+  // smem: mean[B], pivots[B], two chunk buffers of kChunk x B, then the
+  // packed matrices (in the workspace when B is large)
   double* mean = smem;
-  double* vec = mean + B;
-  double* xs = vec + static_cast<size_t>(T) * B;
-  double* A = in_smem ? xs + static_cast<size_t>(kWarps) * B : args.scratch + static_cast<size_t>(f) * 2 * tri(B);
-  double* W = A + tri(B);  // packed L^-1 (lower)
+  double* dv = mean + B;
+  double* vec = dv + B;
+  double* buf = vec + static_cast<size_t>(kChunk) * B;
+  double* A = in_smem ? buf + static_cast<size_t>(kChunk) * B : args.scratch + static_cast<size_t>(f) * 2 * tri(B);
+  double* W = A + tri(B);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) s_flag = 0;
 
   const double N = mom[B + B * B];
   if (!(N > 0.0)) {
@@ -108,32 +184,13 @@ __global__ void __launch_bounds__(kThreads) factor_kernel(const FactorArgs args)
   const double* outer = mom + B;
   for (int i = threadIdx.x; i < B; i += blockDim.x) mean[i] = sum[i] / N;
   __syncthreads();
-  // covariance, loaded (src/linalg.cpp:56-79: correlation then subtract mu mu^T)
-  for (size_t e = threadIdx.x; e < tri(B); e += blockDim.x) {
-    int i = static_cast<int>((sqrt(8.0 * static_cast<double>(e) + 1.0) - 1.0) * 0.5);
-    while (tri(i + 1) <= e) ++i;
-    while (tri(i) > e) --i;
-    const int j = static_cast<int>(e - tri(i));
-    double v = outer[static_cast<size_t>(i) * B + j] / N - mean[i] * mean[j];
-    if (i == j) v += args.loading;
-    A[e] = v;
-  }
-  __syncthreads();
-  if (!cholesky_packed(A, B, &s_flag)) {
+  // covariance, loaded (src/linalg.cpp:56-79), its Cholesky factor and inverse
+  fill_matrix(A, outer, mean, N, args.loading, B, true);
+  if (!cholesky_packed(A, B, dv)) {
     if (threadIdx.x == 0 && args.status) args.status[f] = HSI_E_NOT_POSITIVE_DEFINITE;
     return;
   }
-  // W = L^-1, one column per thread (forward substitution down the column;
-  // src/linalg.cpp:150-162)
-  for (int k = threadIdx.x; k < B; k += blockDim.x) {
-    W[pk(k, k)] = 1.0 / A[pk(k, k)];
-    for (int i = k + 1; i < B; ++i) {
-      double s = 0.0;
-      for (int j = k; j < i; ++j) s -= A[pk(i, j)] * W[pk(j, k)];
-      W[pk(i, k)] = s / A[pk(i, i)];
-    }
-  }
-  __syncthreads();
+  triangular_inverse(A, W, B);
   // outputs: mean, whitener (row-major, upper zero)
   for (int i = threadIdx.x; i < B; i += blockDim.x) {
     if (out64) out64[i] = mean[i];
@@ -141,7 +198,7 @@ __global__ void __launch_bounds__(kThreads) factor_kernel(const FactorArgs args)
   }
   for (size_t e = threadIdx.x; e < static_cast<size_t>(B) * B; e += blockDim.x) {
     const int i = static_cast<int>(e / B), j = static_cast<int>(e % B);
-    const double v = j <= i ? W[pk(i, j)] : 0.0;
+    const double v = j <= i ? W[row_off(i) + j] : 0.0;
     if (out64) out64[B + e] = v;
     if (out32) out32[B + e] = static_cast<float>(v);
   }
@@ -152,81 +209,63 @@ __global__ void __launch_bounds__(kThreads) factor_kernel(const FactorArgs args)
   const size_t off_tw = static_cast<size_t>(B) + static_cast<size_t>(B) * B;
   const size_t off_tn = off_tw + static_cast<size_t>(T) * B;
   const size_t off_cw = off_tn + T;
-  // ACE: u_t = W (d_t - mu), |u_t|^2 -- one warp per target row block
-  for (size_t e = threadIdx.x; e < static_cast<size_t>(T) * B; e += blockDim.x)
-    vec[e] = static_cast<double>(lib[e]) - mean[e % B];
-  __syncthreads();
-  for (int t = warp; t < T; t += kWarps) {
-    const double* c = vec + static_cast<size_t>(t) * B;
-    double norm2 = 0.0;
-    for (int i = 0; i < B; ++i) {
+  // ACE: u_t = W (d_t - mu) and |u_t|^2, kChunk targets at a time
+  for (int t0 = 0; t0 < T; t0 += kChunk) {
+    const int nt = min(kChunk, T - t0);
+    for (int e = threadIdx.x; e < nt * B; e += blockDim.x)
+      vec[e] = static_cast<double>(lib[static_cast<size_t>(t0) * B + e]) - mean[e % B];
+    __syncthreads();
+    lower_matvec(W, vec, buf, B, nt);
+    for (int e = threadIdx.x; e < nt * B; e += blockDim.x) {
+      if (out64) out64[off_tw + static_cast<size_t>(t0) * B + e] = buf[e];
+      if (out32) out32[off_tw + static_cast<size_t>(t0) * B + e] = static_cast<float>(buf[e]);
+    }
+    for (int t = warp; t < nt; t += kWarps) {
       double s = 0.0;
-      for (int j = lane; j <= i; j += 32) s += W[pk(i, j)] * c[j];
+      for (int i = lane; i < B; i += 32) s += buf[t * B + i] * buf[t * B + i];
       s = warp_sum(s);
-      norm2 += s * s;
       if (lane == 0) {
-        if (out64) out64[off_tw + static_cast<size_t>(t) * B + i] = s;
-        if (out32) out32[off_tw + static_cast<size_t>(t) * B + i] = static_cast<float>(s);
+        if (out64) out64[off_tn + t0 + t] = s;
+        if (out32) out32[off_tn + t0 + t] = static_cast<float>(s);
       }
     }
-    if (lane == 0) {
-      if (out64) out64[off_tn + t] = norm2;
-      if (out32) out32[off_tn + t] = static_cast<float>(norm2);
-    }
+    __syncthreads();
   }
-  __syncthreads();
-  // CEM: correlation R = M2/N + loading I, factor into A (reused)
-  if (threadIdx.x == 0) s_flag = 0;
-  for (size_t e = threadIdx.x; e < tri(B); e += blockDim.x) {
-    int i = static_cast<int>((sqrt(8.0 * static_cast<double>(e) + 1.0) - 1.0) * 0.5);
-    while (tri(i + 1) <= e) ++i;
-    while (tri(i) > e) --i;
-    const int j = static_cast<int>(e - tri(i));
-    double v = outer[static_cast<size_t>(i) * B + j] / N;
-    if (i == j) v += args.loading;
-    A[e] = v;
-  }
-  __syncthreads();
-  if (!cholesky_packed(A, B, &s_flag)) {
+  // CEM: R = M2/N + loading I = C C^T; y_t = C^-1 d_t, x_t = C^-T y_t = R^-1 d_t,
+  // d_t . x_t = |y_t|^2; w_t = x_t / |y_t|^2, 0 if that gain is not positive
+  // (src/detector.cpp:128-148)
+  fill_matrix(A, outer, mean, N, args.loading, B, false);
+  if (!cholesky_packed(A, B, dv)) {
     if (threadIdx.x == 0 && args.status) args.status[f] = HSI_E_CORRELATION_NOT_PD;
     return;
   }
-  // x_t = R^-1 d_t by forward then back substitution, one warp per target
-  // (src/linalg.cpp:124-137); the raw target replaces the centred one in vec.
-  for (size_t e = threadIdx.x; e < static_cast<size_t>(T) * B; e += blockDim.x) vec[e] = static_cast<double>(lib[e]);
-  __syncthreads();
-  for (int t = warp; t < T; t += kWarps) {
-    double* x = xs + static_cast<size_t>(warp) * B;
-    const double* d = vec + static_cast<size_t>(t) * B;
-    for (int i = 0; i < B; ++i) {
-      double s = 0.0;
-      for (int k = lane; k < i; k += 32) s += A[pk(i, k)] * x[k];
-      s = warp_sum(s);
-      if (lane == 0) x[i] = (d[i] - s) / A[pk(i, i)];
-      __syncwarp();
+  triangular_inverse(A, W, B);
+  for (int t0 = 0; t0 < T; t0 += kChunk) {
+    const int nt = min(kChunk, T - t0);
+    for (int e = threadIdx.x; e < nt * B; e += blockDim.x)
+      vec[e] = static_cast<double>(lib[static_cast<size_t>(t0) * B + e]);
+    __syncthreads();
+    lower_matvec(W, vec, buf, B, nt);   // y
+    upper_matvec(W, buf, vec, B, nt);   // x (d is no longer needed)
+    for (int t = warp; t < nt; t += kWarps) {
+      double g = 0.0;
+      for (int i = lane; i < B; i += 32) g += buf[t * B + i] * buf[t * B + i];
+      g = warp_sum(g);
+      for (int i = lane; i < B; i += 32) {
+        const double w = g > 0.0 ? vec[t * B + i] / g : 0.0;
+        const size_t o = static_cast<size_t>(t0 + t) * B + i;
+        if (out64) out64[off_cw + o] = w;
+        if (out32) out32[off_cw + o] = static_cast<float>(w);
+        if (cem32) cem32[o] = static_cast<float>(w);
+      }
     }
-    for (int i = B - 1; i >= 0; --i) {
-      double s = 0.0;
-      for (int k = i + 1 + lane; k < B; k += 32) s += A[pk(k, i)] * x[k];
-      s = warp_sum(s);
-      if (lane == 0) x[i] = (x[i] - s) / A[pk(i, i)];
-      __syncwarp();
-    }
-    double g = 0.0;
-    for (int i = lane; i < B; i += 32) g += d[i] * x[i];
-    g = warp_sum(g);
-    for (int i = lane; i < B; i += 32) {
-      const double w = g > 0.0 ? x[i] / g : 0.0;
-      if (out64) out64[off_cw + static_cast<size_t>(t) * B + i] = w;
-      if (out32) out32[off_cw + static_cast<size_t>(t) * B + i] = static_cast<float>(w);
-      if (cem32) cem32[static_cast<size_t>(t) * B + i] = static_cast<float>(w);
-    }
+    __syncthreads();
   }
   if (threadIdx.x == 0 && args.status) args.status[f] = HSI_OK;
 }
 
-size_t smem_bytes(int B, int T) {
-  const size_t vectors = static_cast<size_t>(B) + static_cast<size_t>(T) * B + static_cast<size_t>(kWarps) * B;
+size_t smem_bytes(int B, int /*T*/) {
+  const size_t vectors = 2 * static_cast<size_t>(B) + 2 * static_cast<size_t>(kChunk) * B;
   if (B <= kSmemMaxBands) return sizeof(double) * (vectors + 2 * tri(B));
   return sizeof(double) * vectors;
 }
