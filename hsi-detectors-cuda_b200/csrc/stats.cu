@@ -897,6 +897,26 @@ int encode_cube_map(CUtensorMap* map, const void* cube, int dtype, int64_t pixel
   return r == CUDA_SUCCESS ? HSI_OK : HSI_E_INVALID;
 }
 
+// The same map with the 128-byte swizzle: boxes land in shared memory in the
+// UMMA "128B swizzle" layout (inner box extent must be 128 bytes; destination
+// 1024-byte aligned), ready to be an MMA operand without conversion.
+int encode_cube_map_sw128(CUtensorMap* map, const void* cube, int dtype, int64_t pixels, int bands, int64_t stride,
+                          int box_pixels, int box_bands) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return HSI_E_NO_DEVICE;
+  const size_t esize = dtype == HSI_F32 ? 4 : 2;
+  if (static_cast<size_t>(box_pixels) * esize != 128) return HSI_E_INVALID;
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(pixels), static_cast<cuuint64_t>(bands)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(stride) * esize};
+  const cuuint32_t box[2] = {static_cast<cuuint32_t>(box_pixels), static_cast<cuuint32_t>(box_bands)};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, dtype == HSI_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                        const_cast<void*>(cube), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? HSI_OK : HSI_E_INVALID;
+}
+
 }  // namespace hsi_b200
 
 using namespace hsi_b200;

@@ -141,5 +141,8 @@ __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap* map) {
 // bands).  Returns 0 on success.
 int encode_cube_map(CUtensorMap* map, const void* cube, int dtype, int64_t pixels, int bands, int64_t stride,
                     int box_pixels, int box_bands);
+// Same, with the 128-byte swizzle (box_pixels * element size must be 128).
+int encode_cube_map_sw128(CUtensorMap* map, const void* cube, int dtype, int64_t pixels, int bands, int64_t stride,
+                          int box_pixels, int box_bands);
 
 }  // namespace hsi_b200

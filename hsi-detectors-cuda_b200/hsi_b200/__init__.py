@@ -141,6 +141,17 @@ def _optional_symbols(L):
         "hsi_transpose_bip_to_bsq": ([vp, vp, i32, i32, i32, i64, vp], i32),
         "hsi_accumulate_shifted_moments": ([vp, vp, i32, vp, vp, vp], i32),
         "hsi_detect_noalloc": ([vp, vp, i32, i32, C.c_float, i32, i32, i32, vp, vp, vp], i32),
+        "hsi_screen_param_count": ([i32], i64),
+        "hsi_screen_init": ([vp, i32, C.c_uint64, vp], i32),
+        "hsi_screen_normaliser": ([vp, i32, vp, vp], i32),
+        "hsi_screen_batch": ([vp, vp, i32, i32, i32, vp, C.c_float, C.c_uint64, i32, i32, vp, vp, vp], i32),
+        "hsi_screen_gather": ([vp, i32, i64, i32, vp, vp, i32, vp, vp], i32),
+        "hsi_screen_train_workspace_bytes": ([i32, i32], C.c_size_t),
+        "hsi_screen_gradients": ([vp, i32, vp, vp, i32, C.c_float, vp, vp, vp, C.c_size_t, vp], i32),
+        "hsi_screen_adam": ([vp, vp, vp, i32, C.c_float, i32, vp], i32),
+        "hsi_screen_infer_workspace_bytes": ([i32], C.c_size_t),
+        "hsi_screen_infer": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, vp, C.c_size_t, vp], i32),
+        "hsi_gather_candidates": ([vp, i32, i64, i32, i32, vp, vp, i32, vp, i64, vp], i32),
     }
     for name, (argtypes, restype) in table.items():
         if hasattr(L, name):

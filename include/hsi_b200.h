@@ -299,6 +299,56 @@ HSI_API size_t hsi_detect_batch_workspace_bytes(const hsi_detect_job* jobs, int 
 HSI_API int hsi_detect_batch(const hsi_detect_job* jobs, int num_jobs, void* d_workspace,
                              size_t workspace_bytes, hsi_stream_t stream);
 
+/* ---- learned screen (no counterpart in the reference) --------------------------
+ * A per-pixel MLP B -> 64 -> 32 -> 1 (ReLU; bfloat16 weights, FP32
+ * accumulation) that proposes candidate pixels for the plain ACE detector,
+ * which re-scores every proposal and stays the fallback.  Trained on the
+ * device on the detector's own decisions by the kernels below.
+ * Parameters (FP32 master copy), Bp = bands rounded up to 64:
+ *   W1[64][Bp] | b1[64] | W2[32][64] | b2[32] | w3[32] | b3
+ * Normaliser: 2*Bp floats, per band the mean and a power-of-two scale near
+ * 1/sigma (zero past the bands).  Features: band-major [Bp][n] floats,
+ * (x - mean) * scale rounded to bfloat16. */
+HSI_API int64_t hsi_screen_param_count(int bands);
+/* He-uniform weights from a counter hash (`seed`), zero biases. */
+HSI_API int hsi_screen_init(float* d_params, int bands, uint64_t seed, hsi_stream_t stream);
+/* Normaliser from a frame's raw FP64 moments (hsi_scene_moments). */
+HSI_API int hsi_screen_normaliser(const double* d_moments, int bands, float* d_norm, hsi_stream_t stream);
+/* Training batch of n pixel indices and 0/1 labels (score >= threshold): the
+ * first `num_positive_draws` drawn from a positive list (e.g. hsi_detect of
+ * the score map, radius 0), the rest uniform over the frame. */
+HSI_API int hsi_screen_batch(const hsi_detection* d_positives, const uint32_t* d_positive_count,
+                             int positive_capacity, int height, int width, const float* d_score, float threshold,
+                             uint64_t seed, int num_positive_draws, int n, int32_t* d_index, float* d_labels,
+                             hsi_stream_t stream);
+/* Features of the indexed pixels, [Bp][n]. */
+HSI_API int hsi_screen_gather(const void* d_cube, int dtype, int64_t plane_stride, int bands, const float* d_norm,
+                              const int32_t* d_index, int n, float* d_features, hsi_stream_t stream);
+/* Mean weighted binary cross-entropy on the logit (positives weighted by
+ * pos_weight) and its gradient for every parameter (d_grads, param-count
+ * floats); `d_loss` (nullable) receives the loss. */
+HSI_API size_t hsi_screen_train_workspace_bytes(int bands, int n);
+HSI_API int hsi_screen_gradients(const float* d_params, int bands, const float* d_features, const float* d_labels,
+                                 int n, float pos_weight, float* d_grads, float* d_loss, void* d_workspace,
+                                 size_t workspace_bytes, hsi_stream_t stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) at iteration `step` >= 1;
+ * d_adam_state: 2 * param-count floats, zeroed before the first step. */
+HSI_API int hsi_screen_adam(float* d_params, float* d_adam_state, const float* d_grads, int bands, float lr, int step,
+                            hsi_stream_t stream);
+/* Logit of every pixel of an fp16 cube (tcgen05: layers 1 and 2 on the
+ * tensor cores, the cube read once by TMA as the first layer's operand).
+ * Workspace: hsi_screen_infer_workspace_bytes, 256-byte aligned. */
+HSI_API size_t hsi_screen_infer_workspace_bytes(int bands);
+HSI_API int hsi_screen_infer(const void* d_cube, int height, int width, int bands, int dtype, int64_t plane_stride,
+                             const float* d_norm, const float* d_params, float* d_logits, void* d_workspace,
+                             size_t workspace_bytes, hsi_stream_t stream);
+/* Copy the spectra of candidate pixels (a detection list and its count) into
+ * a compact BSQ cube of `capacity` pixels at `out_stride`, for re-scoring;
+ * slots past the count hold pixel 0. */
+HSI_API int hsi_gather_candidates(const void* d_cube, int dtype, int64_t plane_stride, int bands, int width,
+                                  const hsi_detection* d_candidates, const uint32_t* d_count, int capacity,
+                                  void* d_out, int64_t out_stride, hsi_stream_t stream);
+
 /* ---- data formats ------------------------------------------------------------ */
 
 /* fp32 -> fp16 (round to nearest even) of `count` elements; d_src 16-byte and

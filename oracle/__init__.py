@@ -96,6 +96,10 @@ def fp64_lib():
         lib.orc_demosaic.restype = C.c_int
         lib.orc_scene_spectra.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, f32p, f32p, f32p]
         lib.orc_generate.argtypes = [C.POINTER(SceneSpec), i64, i64, i64, f32p, C.POINTER(C.c_uint8)]
+        lib.orc_mlp_param_count.argtypes = [C.c_int]
+        lib.orc_mlp_param_count.restype = i64
+        lib.orc_mlp.argtypes = [f32p, C.c_int, f32p, f32p, C.c_int, C.c_double, C.c_int, f64p, f64p]
+        lib.orc_mlp.restype = C.c_double
         _fp64 = lib
     return _fp64
 
@@ -421,3 +425,25 @@ def ref_synthetic_frame(h, w, b, num_targets=3, target_radius=5, seed=4242, fram
     ok = ref_lib().ref_synthetic_frame(h, w, b, num_targets, target_radius, seed, frame_index,
                                        _f(cube), _u8(truth), _f(lib))
     return (cube, truth, lib) if ok else None
+
+
+# ---------------------------------------------------------------------------
+# learned screen (per-pixel MLP B -> 64 -> 32 -> 1)
+# ---------------------------------------------------------------------------
+
+def mlp_param_count(bands):
+    return int(fp64_lib().orc_mlp_param_count(bands))
+
+
+def mlp(params, bands, features, labels=None, pos_weight=1.0, round_bf16=True, grads=False):
+    """FP64 forward (and, with labels, loss and gradient) of the screen MLP.
+    features: (n, bands) float32.  Returns (logits, loss, grads or None)."""
+    params = _c(params, np.float32)
+    features = _c(features, np.float32)
+    n = features.shape[0]
+    logits = np.zeros(n, np.float64)
+    g = np.zeros(mlp_param_count(bands), np.float64) if grads else None
+    lab = None if labels is None else _c(labels, np.float32)
+    loss = fp64_lib().orc_mlp(_f(params), bands, _f(features), _f(lab), n, float(pos_weight),
+                              1 if round_bf16 else 0, _d(logits), _d(g))
+    return logits, loss, g

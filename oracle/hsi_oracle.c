@@ -543,3 +543,106 @@ ORC_API void orc_generate(const hsi_scene_spec* spec, int64_t pixel0, int64_t pi
   }
   free(spectra);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Learned screen: per-pixel MLP B -> 64 -> 32 -> 1 (no reference           */
+/* counterpart; the FP64 checker of the device training and inference).      */
+/* ------------------------------------------------------------------------ */
+/*
+ * Parameters (FP32 master copy), with Bp = bands rounded up to 64:
+ *   W1[64][Bp] | b1[64] | W2[32][64] | b2[32] | w3[32] | b3
+ * Forward:  h1 = relu(W1 x + b1), h2 = relu(W2 h1 + b2), z = w3 . h2 + b3.
+ * Loss: mean over samples of w_s (softplus(z) - y z), w_s = pos_weight for
+ * y = 1, else 1 (binary cross-entropy on the logit, positives weighted).
+ * With round_bf16 the weights W1, W2, w3 are rounded to bfloat16 where they
+ * are used and h1 is rounded to bfloat16 before the second layer -- the
+ * device's numerics -- and the backward pass treats those roundings as the
+ * identity (straight-through), like the device.  Features: [n][bands].
+ */
+#define ORC_H1 64
+#define ORC_H2 32
+
+static int orc_bp(int bands) { return (bands + 63) / 64 * 64; }
+
+ORC_API int64_t orc_mlp_param_count(int bands) {
+  return (int64_t)ORC_H1 * orc_bp(bands) + ORC_H1 + ORC_H2 * ORC_H1 + ORC_H2 + ORC_H2 + 1;
+}
+
+/* round-to-nearest-even to bfloat16, returned as a float */
+static double orc_bf16(double v) {
+  float f = (float)v;
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+  memcpy(&f, &u, 4);
+  return (double)f;
+}
+
+static double orc_softplus(double z) { return z > 0.0 ? z + log1p(exp(-z)) : log1p(exp(z)); }
+
+/* logits[n]; returns nothing.  With grads (count doubles, zeroed here) and
+ * labels, also the loss gradient; returns the loss (0 without labels). */
+ORC_API double orc_mlp(const float* params, int bands, const float* features, const float* labels, int n,
+                       double pos_weight, int round_bf16, double* logits, double* grads) {
+  const int B = bands, Bp = orc_bp(bands);
+  const float* W1 = params;
+  const float* b1 = W1 + (int64_t)ORC_H1 * Bp;
+  const float* W2 = b1 + ORC_H1;
+  const float* b2 = W2 + ORC_H2 * ORC_H1;
+  const float* w3 = b2 + ORC_H2;
+  const float* b3 = w3 + ORC_H2;
+  double *gW1 = 0, *gb1 = 0, *gW2 = 0, *gb2 = 0, *gw3 = 0, *gb3 = 0;
+  if (grads) {
+    memset(grads, 0, sizeof(double) * (size_t)orc_mlp_param_count(bands));
+    gW1 = grads;
+    gb1 = gW1 + (int64_t)ORC_H1 * Bp;
+    gW2 = gb1 + ORC_H1;
+    gb2 = gW2 + ORC_H2 * ORC_H1;
+    gw3 = gb2 + ORC_H2;
+    gb3 = gw3 + ORC_H2;
+  }
+#define RW(v) (round_bf16 ? orc_bf16(v) : (double)(v))
+  double loss = 0.0;
+  for (int s = 0; s < n; ++s) {
+    const float* x = features + (int64_t)s * B;
+    double z1[ORC_H1], h1[ORC_H1], z2[ORC_H2], h2[ORC_H2];
+    for (int j = 0; j < ORC_H1; ++j) {
+      double a = b1[j];
+      for (int b = 0; b < B; ++b) a += RW(W1[(int64_t)j * Bp + b]) * (double)x[b];
+      z1[j] = a;
+      h1[j] = a > 0.0 ? a : 0.0;
+      if (round_bf16) h1[j] = orc_bf16(h1[j]);
+    }
+    for (int k = 0; k < ORC_H2; ++k) {
+      double a = b2[k];
+      for (int j = 0; j < ORC_H1; ++j) a += RW(W2[k * ORC_H1 + j]) * h1[j];
+      z2[k] = a;
+      h2[k] = a > 0.0 ? a : 0.0;
+    }
+    double z = b3[0];
+    for (int k = 0; k < ORC_H2; ++k) z += RW(w3[k]) * h2[k];
+    if (logits) logits[s] = z;
+    if (!labels) continue;
+    const double y = labels[s], w = y > 0.5 ? pos_weight : 1.0;
+    loss += w * (orc_softplus(z) - y * z);
+    if (!grads) continue;
+    const double d3 = w * (1.0 / (1.0 + exp(-z)) - y) / n;
+    gb3[0] += d3;
+    double d2[ORC_H2], d1[ORC_H1];
+    for (int k = 0; k < ORC_H2; ++k) {
+      gw3[k] += d3 * h2[k];
+      d2[k] = z2[k] > 0.0 ? d3 * RW(w3[k]) : 0.0;
+      gb2[k] += d2[k];
+      for (int j = 0; j < ORC_H1; ++j) gW2[k * ORC_H1 + j] += d2[k] * h1[j];
+    }
+    for (int j = 0; j < ORC_H1; ++j) {
+      double a = 0.0;
+      for (int k = 0; k < ORC_H2; ++k) a += d2[k] * RW(W2[k * ORC_H1 + j]);
+      d1[j] = z1[j] > 0.0 ? a : 0.0;
+      gb1[j] += d1[j];
+      for (int b = 0; b < B; ++b) gW1[(int64_t)j * Bp + b] += d1[j] * (double)x[b];
+    }
+  }
+#undef RW
+  return labels ? loss / n : 0.0;
+}
