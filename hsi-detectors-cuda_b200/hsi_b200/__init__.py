@@ -443,3 +443,95 @@ def rx_ace(cube, height, width, bands, stats64, num_targets, dtype=F32, stride=N
     check(fn(_ptr(cube), height, width, bands, dtype, stride, _ptr(stats64), num_targets, _ptr(rx), _ptr(ace_best),
              _ptr(ace_target), _ptr(ace_maps), map_stride, _ptr(workspace), workspace.numel(), _stream(stream)),
           "hsi_rx_ace")
+
+
+# ---------------------------------------------------------------------------
+# learned screen
+# ---------------------------------------------------------------------------
+
+def screen_normaliser(moments, bands, out=None, stream=None):
+    """Per-band mean and power-of-two scale (2 * Bp floats) from raw FP64 moments."""
+    torch = _torch()
+    Bp = (bands + 63) // 64 * 64
+    if out is None:
+        out = torch.zeros(2 * Bp, device=moments.device)
+    check(lib().hsi_screen_normaliser(_ptr(moments), bands, _ptr(out), _stream(stream)), "hsi_screen_normaliser")
+    return out
+
+
+class Screen:
+    """Parameters (FP32 master), Adam state and the training / inference calls
+    of the learned screen, all through the C ABI."""
+
+    def __init__(self, bands, seed=1, device="cuda"):
+        torch = _torch()
+        L = lib()
+        self.bands = bands
+        self.count = int(L.hsi_screen_param_count(bands))
+        self.params = torch.zeros(self.count, device=device)
+        check(L.hsi_screen_init(_ptr(self.params), bands, seed, None), "hsi_screen_init")
+        self.adam = torch.zeros(2 * self.count, device=device)
+        self.grads = torch.zeros(self.count, device=device)
+        self.loss = torch.zeros(1, device=device)
+        self.step = 0
+        self._ws = None
+        self._buffers = {}
+
+    def _train_buffers(self, batch, device):
+        torch = _torch()
+        if batch not in self._buffers:
+            Bp = (self.bands + 63) // 64 * 64
+            wb = lib().hsi_screen_train_workspace_bytes(self.bands, batch)
+            self._buffers[batch] = (torch.empty(batch, dtype=torch.int32, device=device),
+                                    torch.empty(batch, device=device), torch.empty((Bp, batch), device=device),
+                                    torch.empty(wb, dtype=torch.uint8, device=device), wb)
+        return self._buffers[batch]
+
+    def train_on(self, cube, height, width, dtype, norm, score, threshold, steps, batch=4096,
+                 positive_fraction=0.25, lr=1e-3, pos_weight=2.0, seed=0, capacity=1 << 16, stream=None):
+        """`steps` Adam steps on one frame: labels are score >= threshold (the
+        plain detector's decision); a quarter of each batch is drawn from its
+        positive list, the rest uniformly.  Returns the last loss (device)."""
+        L = lib()
+        count, pos = detect(score, None, height, width, threshold, 0, HIGHER_IS_BETTER, capacity, stream=stream)
+        idx, lab, feats, ws, wb = self._train_buffers(batch, cube.device)
+        stride = cube.shape[-1]
+        npos = int(batch * positive_fraction)
+        s = _stream(stream)
+        for k in range(steps):
+            check(L.hsi_screen_batch(_ptr(pos), _ptr(count), capacity, height, width, _ptr(score), float(threshold),
+                                     (seed << 20) + k, npos, batch, _ptr(idx), _ptr(lab), s), "hsi_screen_batch")
+            check(L.hsi_screen_gather(_ptr(cube), dtype, stride, self.bands, _ptr(norm), _ptr(idx), batch,
+                                      _ptr(feats), s), "hsi_screen_gather")
+            check(L.hsi_screen_gradients(_ptr(self.params), self.bands, _ptr(feats), _ptr(lab), batch,
+                                         float(pos_weight), _ptr(self.grads), _ptr(self.loss), _ptr(ws), wb, s),
+                  "hsi_screen_gradients")
+            self.step += 1
+            check(L.hsi_screen_adam(_ptr(self.params), _ptr(self.adam), _ptr(self.grads), self.bands, float(lr),
+                                    self.step, s), "hsi_screen_adam")
+        return self.loss
+
+    def logits(self, cube, height, width, norm, out=None, stream=None):
+        """Logit of every pixel of an fp16 cube (tensor-core inference)."""
+        torch = _torch()
+        L = lib()
+        if out is None:
+            out = torch.empty(height * width, device=cube.device)
+        if self._ws is None:
+            self._ws = torch.empty(L.hsi_screen_infer_workspace_bytes(self.bands), dtype=torch.uint8,
+                                   device=cube.device)
+        check(L.hsi_screen_infer(_ptr(cube), height, width, self.bands, F16, cube.shape[-1], _ptr(norm),
+                                 _ptr(self.params), _ptr(out), _ptr(self._ws), self._ws.numel(), _stream(stream)),
+              "hsi_screen_infer")
+        return out
+
+
+def gather_candidates(cube, dtype, bands, width, candidates, count, capacity, out=None, stream=None):
+    """Spectra of a candidate list as a compact BSQ cube (bands x capacity, stride = capacity)."""
+    torch = _torch()
+    if out is None:
+        out = torch.empty((bands, capacity), dtype=cube.dtype, device=cube.device)
+    check(lib().hsi_gather_candidates(_ptr(cube), dtype, cube.shape[-1], bands, width, _ptr(candidates),
+                                      _ptr(count), capacity, _ptr(out), capacity, _stream(stream)),
+          "hsi_gather_candidates")
+    return out
