@@ -519,7 +519,7 @@ int round_filters(int n) {
 }
 
 template <typename T, int KS, int KC>
-int launch_instance(const ScoreParams& p, int max_bands, cudaStream_t stream) {
+int launch_instance(const ScoreParams& p, int max_bands, int ctas_per_sm, cudaStream_t stream) {
   constexpr int kGroups = (KS > 0) + (KC > 0);
   constexpr int kKG = (KS > KC ? KS : KC);
   const SmemLayout L = smem_layout<T>(kGroups, max_bands, kKG);
@@ -536,30 +536,32 @@ int launch_instance(const ScoreParams& p, int max_bands, cudaStream_t stream) {
     if (per_sm < 1) per_sm = 1;
     configured_bytes = static_cast<int>(L.total);
   }
-  const int grid = sm_count() * per_sm;
+  // ctas_per_sm: 0 = as many as fit; otherwise that many (capped at what fits)
+  const int per = ctas_per_sm > 0 && ctas_per_sm < per_sm ? ctas_per_sm : per_sm;
+  const int grid = sm_count() * per;
   kernel<<<grid, threads, L.total, stream>>>(p, max_bands);
   return static_cast<int>(cudaGetLastError());
 }
 
 template <typename T, int KS>
-int dispatch_kc(int kc, const ScoreParams& p, int max_bands, cudaStream_t s) {
+int dispatch_kc(int kc, const ScoreParams& p, int max_bands, int cps, cudaStream_t s) {
   switch (kc) {
-    case 0: if constexpr (KS > 0) return launch_instance<T, KS, 0>(p, max_bands, s); else return HSI_E_INVALID;
-    case 1: return launch_instance<T, KS, 1>(p, max_bands, s);
-    case 4: return launch_instance<T, KS, 4>(p, max_bands, s);
-    case 8: return launch_instance<T, KS, 8>(p, max_bands, s);
-    default: return launch_instance<T, KS, 16>(p, max_bands, s);
+    case 0: if constexpr (KS > 0) return launch_instance<T, KS, 0>(p, max_bands, cps, s); else return HSI_E_INVALID;
+    case 1: return launch_instance<T, KS, 1>(p, max_bands, cps, s);
+    case 4: return launch_instance<T, KS, 4>(p, max_bands, cps, s);
+    case 8: return launch_instance<T, KS, 8>(p, max_bands, cps, s);
+    default: return launch_instance<T, KS, 16>(p, max_bands, cps, s);
   }
 }
 
 template <typename T>
-int dispatch(int ks, int kc, const ScoreParams& p, int max_bands, cudaStream_t s) {
+int dispatch(int ks, int kc, const ScoreParams& p, int max_bands, int cps, cudaStream_t s) {
   switch (ks) {
-    case 0: return dispatch_kc<T, 0>(kc, p, max_bands, s);
-    case 1: return dispatch_kc<T, 1>(kc, p, max_bands, s);
-    case 4: return dispatch_kc<T, 4>(kc, p, max_bands, s);
-    case 8: return dispatch_kc<T, 8>(kc, p, max_bands, s);
-    default: return dispatch_kc<T, 16>(kc, p, max_bands, s);
+    case 0: return dispatch_kc<T, 0>(kc, p, max_bands, cps, s);
+    case 1: return dispatch_kc<T, 1>(kc, p, max_bands, cps, s);
+    case 4: return dispatch_kc<T, 4>(kc, p, max_bands, cps, s);
+    case 8: return dispatch_kc<T, 8>(kc, p, max_bands, cps, s);
+    default: return dispatch_kc<T, 16>(kc, p, max_bands, cps, s);
   }
 }
 
@@ -585,7 +587,7 @@ int pass_count_host(int total, int pass) {
 }
 
 // One launch per pass over the cube; each pass scores up to 16 filters of each kind.
-int run_passes(ScoreParams& p, int dtype, int max_bands, int max_sam, int max_cem, cudaStream_t s) {
+int run_passes(ScoreParams& p, int dtype, int max_bands, int max_sam, int max_cem, int cps, cudaStream_t s) {
   p.dtype = dtype;
   p.max_sam = max_sam;
   p.max_cem = max_cem;
@@ -595,8 +597,8 @@ int run_passes(ScoreParams& p, int dtype, int max_bands, int max_sam, int max_ce
     p.pass = pass;
     const int ks = round_filters(pass_count_host(max_sam, pass));
     const int kc = round_filters(pass_count_host(max_cem, pass));
-    const int rc = dtype == HSI_F32 ? dispatch<float>(ks, kc, p, max_bands, s)
-                                    : dispatch<__half>(ks, kc, p, max_bands, s);
+    const int rc = dtype == HSI_F32 ? dispatch<float>(ks, kc, p, max_bands, cps, s)
+                                    : dispatch<__half>(ks, kc, p, max_bands, cps, s);
     if (rc != HSI_OK) return rc;
   }
   return HSI_OK;
@@ -624,7 +626,21 @@ extern "C" HSI_API int hsi_score_frames(const hsi_frame* frames, int num_frames,
     max_sam = frames[i].num_sam > max_sam ? frames[i].num_sam : max_sam;
     max_cem = frames[i].num_cem > max_cem ? frames[i].num_cem : max_cem;
   }
-  return run_passes(p, dtype, max_bands, max_sam, max_cem, reinterpret_cast<cudaStream_t>(stream));
+  return run_passes(p, dtype, max_bands, max_sam, max_cem, 0, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" HSI_API int hsi_score_frames_device_grid(const hsi_frame* d_frames, int num_frames, int dtype,
+                                                    int max_bands, int max_sam, int max_cem, int* d_status,
+                                                    int ctas_per_sm, hsi_stream_t stream) {
+  if (!d_frames || num_frames <= 0 || num_frames > kMaxTableFrames || ctas_per_sm < 0) return HSI_E_INVALID;
+  if (max_bands <= 0 || max_bands > HSI_MAX_BANDS || max_sam < 0 || max_cem < 0 || max_sam + max_cem == 0)
+    return HSI_E_INVALID;
+  if (dtype != HSI_F32 && dtype != HSI_F16) return HSI_E_INVALID;
+  ScoreParams p{};
+  p.table = d_frames;
+  p.num_frames = num_frames;
+  p.status = d_status;
+  return run_passes(p, dtype, max_bands, max_sam, max_cem, ctas_per_sm, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" HSI_API int hsi_score_frames_device(const hsi_frame* d_frames, int num_frames, int dtype,
@@ -638,5 +654,5 @@ extern "C" HSI_API int hsi_score_frames_device(const hsi_frame* d_frames, int nu
   p.table = d_frames;
   p.num_frames = num_frames;
   p.status = d_status;
-  return run_passes(p, dtype, max_bands, max_sam, max_cem, reinterpret_cast<cudaStream_t>(stream));
+  return run_passes(p, dtype, max_bands, max_sam, max_cem, 0, reinterpret_cast<cudaStream_t>(stream));
 }

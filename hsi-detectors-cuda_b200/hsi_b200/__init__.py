@@ -535,3 +535,152 @@ def gather_candidates(cube, dtype, bands, width, candidates, count, capacity, ou
                                       _ptr(count), capacity, _ptr(out), capacity, _stream(stream)),
           "hsi_gather_candidates")
     return out
+
+
+# ---------------------------------------------------------------------------
+# batched frame runner (libhsi_cxx.so, include/hsi_batch.h)
+# ---------------------------------------------------------------------------
+
+CXX_LIB_PATH = os.path.join(os.path.dirname(LIB_PATH), "libhsi_cxx.so")
+_cxx = None
+
+
+class BatchFrame(C.Structure):
+    _fields_ = [("cube", C.c_void_p), ("raw", C.c_void_p), ("raw_height", C.c_int32), ("raw_width", C.c_int32),
+                ("period", C.c_int32), ("height", C.c_int32), ("width", C.c_int32), ("bands", C.c_int32),
+                ("dtype", C.c_int32), ("targets", C.c_void_p), ("num_targets", C.c_int32)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("sam_threshold", C.c_float), ("ace_threshold", C.c_float), ("rx_false_alarm_rate", C.c_double),
+                ("loading", C.c_double), ("nms_radius", C.c_int32), ("capacity", C.c_int32),
+                ("autotune", C.c_int32)]
+
+
+class BatchOutputs(C.Structure):
+    _fields_ = [("sam_best", C.c_void_p), ("sam_target", C.c_void_p), ("rx", C.c_void_p), ("ace_best", C.c_void_p),
+                ("ace_target", C.c_void_p), ("detections", C.c_void_p * 3), ("counts", C.c_void_p),
+                ("status", C.c_void_p), ("rx_threshold", C.c_float)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("score_ctas_per_sm", C.c_int32), ("tensor_core_rx_frames", C.c_int32),
+                ("plain_rx_frames", C.c_int32), ("tuning_ms", C.c_float)]
+
+
+def cxx_lib():
+    """libhsi_cxx.so (C++ API and the batch runner's C ABI); raises if not built."""
+    global _cxx
+    if _cxx is None:
+        lib()  # the kernels library first (libhsi_cxx links it)
+        if not os.path.exists(CXX_LIB_PATH):
+            raise RuntimeError(f"{CXX_LIB_PATH} is missing: build it with `make -C {PKG}`")
+        L = C.CDLL(CXX_LIB_PATH)
+        vp, i32 = C.c_void_p, C.c_int
+        L.hsi_batch_create.argtypes = [C.POINTER(BatchFrame), i32, C.POINTER(BatchOptions), C.POINTER(C.c_int)]
+        L.hsi_batch_create.restype = vp
+        for name in ("hsi_batch_run", "hsi_batch_capture", "hsi_batch_launch"):
+            getattr(L, name).argtypes = [vp, vp]
+            getattr(L, name).restype = i32
+        L.hsi_batch_outputs_of.argtypes = [vp, i32, C.POINTER(BatchOutputs)]
+        L.hsi_batch_outputs_of.restype = i32
+        L.hsi_batch_tuning_of.argtypes = [vp, C.POINTER(BatchTuning)]
+        L.hsi_batch_tuning_of.restype = i32
+        L.hsi_batch_destroy.argtypes = [vp]
+        L.hsi_batch_destroy.restype = None
+        _cxx = L
+    return _cxx
+
+
+class Batch:
+    """A batch of uneven frames run by the library's batched plan.  `frames`:
+    dicts with cube (device BSQ tensor at plane_stride) or raw (device mosaic,
+    with period), height, width, bands, dtype, targets (numpy T x B float32)."""
+
+    def __init__(self, frames, sam_threshold=0.10, ace_threshold=0.5, rx_false_alarm_rate=1e-3, loading=1e-6,
+                 nms_radius=2, capacity=4096, autotune=True):
+        import numpy as np
+        L = cxx_lib()
+        self._keep = []
+        arr = (BatchFrame * len(frames))()
+        for i, f in enumerate(frames):
+            tg = np.ascontiguousarray(f["targets"], np.float32)
+            self._keep.append(tg)
+            raw = f.get("raw")
+            cube = f.get("cube")
+            arr[i] = BatchFrame(cube.data_ptr() if cube is not None else None,
+                                raw.data_ptr() if raw is not None else None,
+                                raw.shape[0] if raw is not None else 0, raw.shape[1] if raw is not None else 0,
+                                f.get("period", 0), f.get("height", 0), f.get("width", 0), f["bands"],
+                                f.get("dtype", F32), tg.ctypes.data, tg.shape[0])
+        opt = BatchOptions(sam_threshold, ace_threshold, rx_false_alarm_rate, loading, nms_radius, capacity,
+                           1 if autotune else 0)
+        st = C.c_int(0)
+        self.handle = L.hsi_batch_create(arr, len(frames), C.byref(opt), C.byref(st))
+        check(st.value, "hsi_batch_create")
+        self.frames = frames
+        self.capacity = capacity
+
+    def run(self, stream=None):
+        check(cxx_lib().hsi_batch_run(self.handle, _stream(stream)), "hsi_batch_run")
+
+    def capture(self, stream):
+        check(cxx_lib().hsi_batch_capture(self.handle, _stream(stream)), "hsi_batch_capture")
+
+    def launch(self, stream):
+        check(cxx_lib().hsi_batch_launch(self.handle, _stream(stream)), "hsi_batch_launch")
+
+    def outputs(self, i):
+        o = BatchOutputs()
+        check(cxx_lib().hsi_batch_outputs_of(self.handle, i, C.byref(o)), "hsi_batch_outputs_of")
+        return o
+
+    def tuning(self):
+        t = BatchTuning()
+        check(cxx_lib().hsi_batch_tuning_of(self.handle, C.byref(t)), "hsi_batch_tuning_of")
+        return {"score_ctas_per_sm": t.score_ctas_per_sm, "tensor_core_rx_frames": t.tensor_core_rx_frames,
+                "plain_rx_frames": t.plain_rx_frames, "tuning_ms": round(t.tuning_ms, 2)}
+
+    def close(self):
+        if self.handle:
+            cxx_lib().hsi_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def device_copy(ptr, n, dtype, device="cuda"):
+    """A new torch tensor holding n elements copied from device memory at `ptr`
+    (memory the library owns, e.g. a batch's outputs)."""
+    torch = _torch()
+    t = torch.empty(n, dtype=dtype, device=device)
+    rt = _cudart()
+    err = rt.cudaMemcpy(C.c_void_p(t.data_ptr()), C.c_void_p(ptr), t.numel() * t.element_size(), 4)  # Default
+    if err != 0:
+        raise HsiError(err, "cudaMemcpy")
+    return t
+
+
+_rt = None
+
+
+def _cudart():
+    """The CUDA runtime the library is linked against (already loaded)."""
+    global _rt
+    if _rt is None:
+        lib()
+        for name in ("libcudart.so.12", "libcudart.so"):
+            try:
+                _rt = C.CDLL(name)
+                break
+            except OSError:
+                continue
+        if _rt is None:
+            raise RuntimeError("the CUDA runtime library is not loadable")
+        _rt.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+        _rt.cudaMemcpy.restype = C.c_int
+    return _rt

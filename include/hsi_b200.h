@@ -172,6 +172,12 @@ HSI_API int hsi_score_frames(const hsi_frame* frames, int num_frames, hsi_stream
 #define HSI_MAX_TABLE_FRAMES 256
 HSI_API int hsi_score_frames_device(const hsi_frame* d_frames, int num_frames, int dtype, int max_bands,
                                     int max_sam, int max_cem, int* d_status, hsi_stream_t stream);
+/* The same with the persistent grid chosen by the caller: `ctas_per_sm`
+ * CTAs per SM (0: as many as fit, the default above; larger values are
+ * capped at what fits).  The autotuner's knob (hsi::BatchRunner). */
+HSI_API int hsi_score_frames_device_grid(const hsi_frame* d_frames, int num_frames, int dtype, int max_bands,
+                                         int max_sam, int max_cem, int* d_status, int ctas_per_sm,
+                                         hsi_stream_t stream);
 
 /* ---- scene statistics -------------------------------------------------------
  * Raw first and second moments of one frame.  Output `d_moments` (FP64):

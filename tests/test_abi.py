@@ -1,4 +1,6 @@
-"""The C-ABI library loads and exports every entry point include/*.h declares.
+"""The C-ABI libraries load and export every entry point include/*.h declares:
+include/hsi_b200.h from libhsi_b200.so (kernels), include/hsi_batch.h from
+libhsi_cxx.so (the batch runner, host C++ over the first).
 
 No compute calls: these run without a GPU."""
 import ctypes as C
@@ -10,11 +12,15 @@ import pytest
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(REPO, "hsi-detectors-cuda_b200", "hsi_b200", "libhsi_b200.so")
+CXXLIB = os.path.join(REPO, "hsi-detectors-cuda_b200", "hsi_b200", "libhsi_cxx.so")
+LIB_OF_HEADER = {"hsi_b200.h": LIB, "hsi_batch.h": CXXLIB}
 
 
-def declared_symbols():
+def declared_symbols(header=None):
     names = set()
     for h in glob.glob(os.path.join(REPO, "include", "*.h")):
+        if header and os.path.basename(h) != header:
+            continue
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"HSI_API\s+[\w\s\*]+?\b(hsi_\w+)\s*\(", text):
@@ -27,11 +33,19 @@ def test_header_declares_entry_points():
     assert "hsi_score_frames" in names and "hsi_detect" in names and len(names) >= 9
 
 
-def test_library_exports_every_declared_symbol():
-    if not os.path.exists(LIB):
-        pytest.fail(f"{LIB} not built (run `make -C hsi-detectors-cuda_b200`)")
-    lib = C.CDLL(LIB)
-    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+def test_every_header_is_mapped_to_its_library():
+    headers = {os.path.basename(h) for h in glob.glob(os.path.join(REPO, "include", "*.h"))}
+    assert headers == set(LIB_OF_HEADER)
+
+
+@pytest.mark.parametrize("header", sorted(LIB_OF_HEADER))
+def test_library_exports_every_declared_symbol(header):
+    path = LIB_OF_HEADER[header]
+    if not os.path.exists(path):
+        pytest.fail(f"{path} not built (run `make -C hsi-detectors-cuda_b200`)")
+    C.CDLL(LIB)  # libhsi_cxx resolves against it
+    lib = C.CDLL(path)
+    missing = [n for n in declared_symbols(header) if not hasattr(lib, n)]
     assert not missing, f"declared but not exported: {missing}"
 
 
