@@ -48,6 +48,27 @@ LOADING = 1e-6
 CEM_THRESHOLD = 0.5
 
 
+def max_over_ranks(dist, values, device):
+    """Element-wise max of per-rank timings over all ranks (every rank gets it):
+    the multi-GPU step time is the slowest rank's."""
+    import torch
+    if dist is None:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def whole_job_mpix(world, pixels_per_rank, ms):
+    """Whole-job throughput: every rank processes its own frames (weak scaling)."""
+    return world * pixels_per_rank / (ms / 1e3) / 1e6
+
+
+def rank_seed(base, rank, stride=1000):
+    """Frame seeds per rank: ranks score different frames of the same scene model."""
+    return base + stride * rank
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -367,7 +388,7 @@ def run_ours(args, workload):
     torch.cuda.set_device(device)
     hsi.lib()
 
-    wl = Workload(hsi, torch, args.frames, workload, device, seed_base=0x5EED1000 + 1000 * rank)
+    wl = Workload(hsi, torch, args.frames, workload, device, seed_base=rank_seed(0x5EED1000, rank))
     stream = torch.cuda.current_stream(device)
 
     def barrier():
@@ -397,12 +418,9 @@ def run_ours(args, workload):
     ms = start.elapsed_time(end) / args.steps
     kernel_ms = float(np.mean([a.elapsed_time(b) for a, b, _ in kev]))
     stats_ms = float(np.mean([c.elapsed_time(a) for a, _, c in kev]))
-    if world > 1:
-        t = torch.tensor([ms, kernel_ms, stats_ms], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, kernel_ms, stats_ms = float(t[0]), float(t[1]), float(t[2])
+    ms, kernel_ms, stats_ms = max_over_ranks(dist if world > 1 else None, [ms, kernel_ms, stats_ms], device)
     pixels_step = args.frames * H * W
-    value = world * pixels_step / (ms / 1e3) / 1e6
+    value = whole_job_mpix(world, pixels_step, ms)
 
     # dominant kernel: the fused scoring pass
     peaks = {}
@@ -537,9 +555,7 @@ def run_e2e(hsi, torch, wl, stream, args, world):
     ms = start.elapsed_time(end) / args.steps
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([ms], device=stream.device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t[0])
+        ms = max_over_ranks(dist, [ms], stream.device)[0]
     value = world * args.frames * H * W / (ms / 1e3) / 1e6
     h2d = args.frames * host[0].numel() * host[0].element_size()
     d2h = out_host.numel() * 4 + count_host.numel() * 4
@@ -591,7 +607,7 @@ def run_rxace(args):
     H, Wd, T = RX_H, RX_W, TARGETS
     P = H * Wd
     sc = hsi.scene(B, n_targets=T, target_frac=0.002, anomaly_frac=0.001, library_seed=0x5EED2000,
-                   frame_seed=0x5EED2001 + rank)
+                   frame_seed=rank_seed(0x5EED2001, rank))
     cube, _ = hsi.generate(sc, H, Wd, truth=False, device=device)
     stride = hsi.plane_stride(H, Wd)
     lib = torch.from_numpy(hsi.scene_targets(sc)).to(device)
@@ -649,10 +665,7 @@ def run_rxace(args):
     with ClockSampler(uuid) as clocks:
         ms, kern_ms = timed(False, args.steps, args.warmup)
     plain_ms, plain_kern = timed(True, max(2, args.steps // 2), 1)
-    if dist:
-        t = torch.tensor([ms, kern_ms, plain_ms, plain_kern], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, kern_ms, plain_ms, plain_kern = [float(v) for v in t]
+    ms, kern_ms, plain_ms, plain_kern = max_over_ranks(dist, [ms, kern_ms, plain_ms, plain_kern], device)
 
     # error of the measured path against a torch FP64 reference (first 64 rows)
     statistics(cube)
@@ -805,7 +818,7 @@ def run_screen(args):
     H, Wd = SCR_H, SCR_W
     P = H * Wd
     sc = hsi.scene(Bs, n_targets=T, target_frac=0.002, anomaly_frac=0.001, library_seed=lib_seed,
-                   frame_seed=0x5EED5900 + rank)
+                   frame_seed=rank_seed(0x5EED5900, rank))
     cube, _ = hsi.generate(sc, H, Wd, dtype=1, truth=False, device=device)
     stride = cube.shape[-1]
     moments = torch.zeros(Bs + Bs * Bs + 1, dtype=torch.float64, device=device)
@@ -903,10 +916,8 @@ def run_screen(args):
     ev[1].record(stream)
     torch.cuda.synchronize()
     screen_ms = ev[0].elapsed_time(ev[1])
-    if dist:
-        t = torch.tensor([ms, plain_ms, screen_ms, score_ms, plain_score_ms], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, plain_ms, screen_ms, score_ms, plain_score_ms = [float(v) for v in t]
+    ms, plain_ms, screen_ms, score_ms, plain_score_ms = max_over_ranks(
+        dist, [ms, plain_ms, screen_ms, score_ms, plain_score_ms], device)
 
     # quality against plain ACE on the whole frame
     screen_step(cube)
@@ -1005,7 +1016,7 @@ def run_batch(args):
     frames, pixels, cube_bytes = [], 0, 0
     for i, (h, w, b, t, mosaic) in enumerate(specs):
         sc = hsi.scene(b, n_targets=t, target_frac=0.003, anomaly_frac=0.001, library_seed=0x5EED7100 + i,
-                       frame_seed=0x5EED7200 + 64 * rank + i)
+                       frame_seed=rank_seed(0x5EED7200, rank) + i)
         cube, _ = hsi.generate(sc, h, w, truth=False, device=device)
         targets = hsi.scene_targets(sc)
         if mosaic:
@@ -1047,10 +1058,7 @@ def run_batch(args):
     with ClockSampler(uuid) as clocks:
         ms = timed(batch.launch, args.steps)
     eager_ms = timed(batch.run, max(2, args.steps // 2))
-    if dist:
-        t = torch.tensor([ms, eager_ms], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, eager_ms = float(t[0]), float(t[1])
+    ms, eager_ms = max_over_ranks(dist, [ms, eager_ms], device)
     tuning = batch.tuning()
     # launches per run: demosaic, moments (6 tensor-core / 3 plain), factor, RX/ACE (prep + main per pass),
     # one scorer launch, the counts memset, three detection launches per 64 lists
