@@ -52,6 +52,7 @@ struct hsi_batch {
   size_t det_bytes = 0;
   uint32_t* all_counts = nullptr;
   std::vector<hsi_detect_job> jobs;
+  std::vector<hsi_moments_job> moment_jobs;  // every frame's moments in one batched call
   hsi_frame* table[2] = {nullptr, nullptr};
   int table_n[2] = {0, 0}, table_bands[2] = {0, 0}, table_targets[2] = {0, 0};
   int32_t* score_status = nullptr;
@@ -100,19 +101,21 @@ struct hsi_batch {
     const hsi_stream_t hs = reinterpret_cast<hsi_stream_t>(s);
     for (Frame& f : frames) {
       const hsi_batch_frame& sp = f.spec;
-      int rc = HSI_OK;
-      if (sp.raw)
-        rc = hsi_demosaic(sp.raw, sp.raw_height, sp.raw_width, sp.period, sp.bands, nullptr, f.cube, HSI_F32, f.stride,
-                          hs);
-      if (rc == HSI_OK)
-        rc = hsi_scene_moments(f.cube, sp.height, sp.width, sp.bands, sp.dtype, f.stride, f.moments, nullptr,
-                               stats_ws, stats_bytes, hs);
-      if (rc == HSI_OK)
-        rc = hsi_build_statistics(1, sp.bands, sp.num_targets, opt.loading, f.moments, f.targets, 0, f.stats64,
-                                  nullptr, nullptr, f.status, factor_ws, factor_bytes, hs);
+      if (!sp.raw) continue;
+      const int rc = hsi_demosaic(sp.raw, sp.raw_height, sp.raw_width, sp.period, sp.bands, nullptr, f.cube, HSI_F32,
+                                  f.stride, hs);
       if (rc != HSI_OK) return rc;
     }
-    int rc = score(score_ctas_per_sm, s);
+    int rc = hsi_scene_moments_batch(moment_jobs.data(), static_cast<int>(moment_jobs.size()), stats_ws, stats_bytes,
+                                     hs);
+    if (rc != HSI_OK) return rc;
+    for (Frame& f : frames) {
+      const hsi_batch_frame& sp = f.spec;
+      rc = hsi_build_statistics(1, sp.bands, sp.num_targets, opt.loading, f.moments, f.targets, 0, f.stats64, nullptr,
+                                nullptr, f.status, factor_ws, factor_bytes, hs);
+      if (rc != HSI_OK) return rc;
+    }
+    rc = score(score_ctas_per_sm, s);
     if (rc != HSI_OK) return rc;
     for (Frame& f : frames) {
       rc = rx_ace(f, f.tensor_core_rx, s);
@@ -202,7 +205,16 @@ int build(hsi_batch* bt, const hsi_batch_frame* frames, int n) {
     if (e != cudaSuccess) return static_cast<int>(e);
     f.rx_threshold = static_cast<float>(hsi::rx_threshold_for_false_alarm_rate(B, o.rx_false_alarm_rate));
     f.tensor_core_rx = B <= 127;
-    bt->stats_bytes = std::max(bt->stats_bytes, hsi_stats_workspace_bytes(sp.height, sp.width, B));
+    hsi_moments_job mj;
+    std::memset(&mj, 0, sizeof(mj));
+    mj.cube = f.cube;
+    mj.plane_stride = f.stride;
+    mj.moments = f.moments;
+    mj.height = sp.height;
+    mj.width = sp.width;
+    mj.bands = B;
+    mj.dtype = sp.dtype;
+    bt->moment_jobs.push_back(mj);
     bt->factor_bytes = std::max(bt->factor_bytes, hsi_factor_workspace_bytes(1, B));
     rx_bytes = std::max(rx_bytes, std::max(hsi_rx_ace_workspace_bytes(B, T), hsi_rx_ace_simt_workspace_bytes(B, T)));
     hsi_frame hf;
@@ -262,6 +274,7 @@ int build(hsi_batch* bt, const hsi_batch_frame* frames, int n) {
     bt->det_bytes = std::max(bt->det_bytes, hsi_detect_batch_workspace_bytes(&bt->jobs[j0], m));
   }
   bt->rx_bytes = rx_bytes;
+  bt->stats_bytes = hsi_scene_moments_batch_workspace_bytes(bt->moment_jobs.data(), n);
   unsigned char* p = nullptr;
   rc = bt->alloc(&p, std::max<size_t>(bt->stats_bytes, 256));
   bt->stats_ws = p;

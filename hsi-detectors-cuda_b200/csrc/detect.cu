@@ -27,6 +27,10 @@ constexpr int kPerThread = 8;
 constexpr int kSeg = kThreads * kPerThread;  // 2048 pixels per segment
 constexpr int kWordsPerSeg = kSeg / 32;      // 64
 constexpr int kMaxStagedRadius = 4;
+constexpr int kColsPerThread = (kSeg + 2 * kMaxStagedRadius + kThreads - 1) / kThreads;  // 9
+// Segments with at most this many threads holding a candidate skip the staged
+// window and read their candidates' neighbourhoods from global memory.
+constexpr int kSparseThreads = 64;
 constexpr int kMaxJobs = 64;
 
 struct Job {
@@ -63,6 +67,17 @@ __device__ __forceinline__ int find_job(const Batch& b, int seg) {
 
 __device__ __forceinline__ bool better(float a, float b, bool higher) { return higher ? a > b : a < b; }
 
+// The total order of the suppression window: the better score first (by
+// polarity), then the lower linear index; NaN (outside the frame) is last.
+// A candidate survives exactly when it is the first of its window.  Inside a
+// staged window the position ry * tw + c orders pixels as their linear
+// indices do (row first, c < tw), so it stands in for the index.
+__device__ __forceinline__ bool lex_first(float av, int ai, float bv, int bi, bool higher) {
+  if (isnan(bv)) return !isnan(av);
+  if (isnan(av)) return false;
+  return better(av, bv, higher) || (av == bv && ai < bi);
+}
+
 // NMS against global memory, for radii too large to stage.
 __device__ bool local_best_global(const float* __restrict__ s, int x, int y, int w, int h, int r, float self,
                                   bool higher) {
@@ -84,7 +99,9 @@ __device__ bool local_best_global(const float* __restrict__ s, int x, int y, int
 }
 
 __global__ void __launch_bounds__(kThreads) flags_kernel(const __grid_constant__ Batch b) {
-  extern __shared__ float tile[];  // (2r+1) rows x (kSeg + 2r) columns
+  // (2r+1) rows x (kSeg + 2r) columns of scores (at least 3 rows: after the
+  // vertical pass rows 0 and 1 hold each column's best value and index)
+  extern __shared__ float tile[];
   __shared__ uint32_t s_count[kThreads / 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int seg = blockIdx.x; seg < b.total_segs; seg += gridDim.x) {
@@ -98,15 +115,68 @@ __global__ void __launch_bounds__(kThreads) flags_kernel(const __grid_constant__
     const bool staged = r <= kMaxStagedRadius;
     const bool higher = J.higher != 0;
     const int tw = kSeg + 2 * r;
-    if (r > 0 && staged) {
-      const int rows = 2 * r + 1;
-      for (int e = threadIdx.x; e < rows * (len + 2 * r); e += kThreads) {
-        const int ry = e / (len + 2 * r), rx = e % (len + 2 * r);
-        const int gy = y - r + ry, gx = x0 - r + rx;
-        float v = __int_as_float(0x7fc00000);  // NaN: never better, never equal
-        if (gy >= 0 && gy < J.height && gx >= 0 && gx < J.width)
-          v = J.score[static_cast<int64_t>(gy) * J.width + gx];
-        tile[ry * tw + rx] = v;
+    float* col_v = tile;                               // tile row 0, after the vertical pass
+    int* col_i = reinterpret_cast<int*>(tile + tw);    // tile row 1
+    // threshold first: a segment with few candidates checks their windows in
+    // global memory (L1/L2), one with many stages the whole window once
+    float sv[kPerThread];
+    uint32_t over_bits = 0;
+#pragma unroll
+    for (int i = 0; i < kPerThread; ++i) {
+      const int xi = i * kThreads + threadIdx.x;
+      sv[i] = 0.0f;
+      if (xi < len) {
+        sv[i] = J.score[static_cast<int64_t>(y) * J.width + x0 + xi];
+        if (higher ? (sv[i] >= J.threshold) : (sv[i] <= J.threshold)) over_bits |= 1u << i;
+      }
+    }
+    const int busy = __syncthreads_count(over_bits != 0);  // threads holding a candidate
+    const bool use_tile = r > 0 && staged && busy > kSparseThreads;
+    if (use_tile) {
+      // row by row, no index division; NaN outside the frame: never better, never equal
+      const float nan = __int_as_float(0x7fc00000);
+      for (int ry = 0; ry <= 2 * r; ++ry) {
+        const int gy = y - r + ry;
+        const bool row_in = gy >= 0 && gy < J.height;
+        const float* src = J.score + static_cast<int64_t>(row_in ? gy : 0) * J.width;
+        float* dst = tile + ry * tw;
+        for (int rx = threadIdx.x; rx < len + 2 * r; rx += kThreads) {
+          const int gx = x0 - r + rx;
+          dst[rx] = row_in && gx >= 0 && gx < J.width ? src[gx] : nan;
+        }
+      }
+      __syncthreads();
+      // vertical pass: the first (score, index) of each staged column, kept in
+      // registers until every thread has read the tile, then written over its
+      // first two rows
+      float cv[kColsPerThread];
+      int ci[kColsPerThread];
+#pragma unroll
+      for (int k = 0; k < kColsPerThread; ++k) {
+        const int c = threadIdx.x + k * kThreads;
+        cv[k] = __int_as_float(0x7fc00000);
+        ci[k] = 0;
+        if (c < len + 2 * r) {
+          cv[k] = tile[c];
+          ci[k] = c;
+          for (int ry = 1; ry <= 2 * r; ++ry) {
+            const int id = ry * tw + c;
+            const float v = tile[id];
+            if (lex_first(v, id, cv[k], ci[k], higher)) {
+              cv[k] = v;
+              ci[k] = id;
+            }
+          }
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kColsPerThread; ++k) {
+        const int c = threadIdx.x + k * kThreads;
+        if (c < len + 2 * r) {
+          col_v[c] = cv[k];
+          col_i[c] = ci[k];
+        }
       }
       __syncthreads();
     }
@@ -115,29 +185,27 @@ __global__ void __launch_bounds__(kThreads) flags_kernel(const __grid_constant__
     for (int i = 0; i < kPerThread; ++i) {
       const int xi = i * kThreads + threadIdx.x;  // pixel within the segment
       bool pass = false;
-      if (xi < len) {
+      if ((over_bits >> i) & 1u) {
         const int x = x0 + xi;
-        const float s = J.score[static_cast<int64_t>(y) * J.width + x];
-        const bool over = higher ? (s >= J.threshold) : (s <= J.threshold);
-        if (over) {
-          if (r == 0) {
-            pass = true;
-          } else if (staged) {
-            pass = true;
-            const float* c = tile + r * tw + (xi + r);  // centre of the window
-            for (int dy = -r; dy <= r && pass; ++dy) {
-              for (int dx = -r; dx <= r; ++dx) {
-                if (dx == 0 && dy == 0) continue;
-                const float o = c[dy * tw + dx];
-                if (better(o, s, higher) || (o == s && (dy < 0 || (dy == 0 && dx < 0)))) {
-                  pass = false;
-                  break;
-                }
-              }
+        const float s = sv[i];
+        if (r == 0) {
+          pass = true;
+        } else if (use_tile) {
+          // first of the window = first of the column bests around it
+          const int self = r * tw + xi + r;  // tile position of the candidate
+          float bv = s;
+          int bi = self;
+          for (int dx = -r; dx <= r; ++dx) {
+            const float v = col_v[xi + r + dx];
+            const int id = col_i[xi + r + dx];
+            if (lex_first(v, id, bv, bi, higher)) {
+              bv = v;
+              bi = id;
             }
-          } else {
-            pass = local_best_global(J.score, x, y, J.width, J.height, r, s, higher);
           }
+          pass = bi == self;
+        } else {
+          pass = local_best_global(J.score, x, y, J.width, J.height, r, s, higher);
         }
       }
       const uint32_t word = __ballot_sync(0xffffffffu, pass);
@@ -296,7 +364,7 @@ int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cuda
   b.counts = p;
   b.offsets = p + segs;
   b.masks = p + 2 * segs;
-  const size_t smem = static_cast<size_t>(2 * max_r + 1) * (kSeg + 2 * max_r) * sizeof(float);
+  const size_t smem = static_cast<size_t>(2 * (max_r > 0 ? max_r : 1) + 1) * (kSeg + 2 * max_r) * sizeof(float);
   static bool configured = false;
   if (!configured) {
     const cudaError_t e = cudaFuncSetAttribute(flags_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

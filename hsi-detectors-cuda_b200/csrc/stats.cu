@@ -1,6 +1,6 @@
 // stats.cu - scene moments on the 5th-generation tensor cores, exactly.
 //
-// Computes, for one BSQ frame, the raw first and second moments the detector
+// Computes, for BSQ frames, the raw first and second moments the detector
 // statistics are built from (reference: SpectralMoments, include/hsi/linalg.hpp
 // :22-51, accumulated by src/detectors_cpu.cpp:77-93 on the CPU and by the
 // never-called src/stats.cu:72-165 on the GPU).
@@ -14,32 +14,51 @@
 // exactly.  So:
 //   d = x - r (r: per-band reference near the mean, as the reference's shifted
 //   accumulation, include/hsi/linalg.hpp:53-90), fixed point
-//   q = rint(d * 2^e_b) with |q| < 2^22 (e_b from a subsample with 4x headroom;
-//   an overflow re-runs the pass with the observed range), balanced signed
-//   8-bit limbs q = L0*2^16 + L1*2^8 + L2, and four exact INT32 accumulators
-//     A0 = sum L0 L0^T,  A1 = sum L0 L1^T,  A2 = sum (L1 L1^T + 2 L0 L2^T),
-//     A3 = sum 2 L1 L2^T
-//   (tcgen05.mma kind::i8, seven MMAs per K-step).  F = 2^32 A0 + 2^25 A1 +
-//   2^16 A2 + 2^8 A3 in FP64 and S = (F + F^T)/2 is sum q q^T except the
-//   weight-1 products L2 L2^T: their diagonal is added back exactly (the
-//   converters count sum L2^2 per band), their off-diagonal sums are those of
-//   independent rounding residues.  The cross terms matter: when outliers set
-//   the fixed-point range, typical q carry only ~15 significant bits.
+//   q = rint(d * 2^e_b) with -2^22 - 2^15 - 2^7 <= q < 2^22 - 2^15 - 2^7
+//   (e_b from a subsample with 4x headroom; a value out of range re-runs the
+//   pass with the observed range), balanced signed 8-bit limbs
+//   q = L0*2^16 + L1*2^8 + L2 with L0 in [-64, 63], so that D = 2 L0 is an
+//   INT8 too, and four exact INT32 accumulators
+//     A0 = sum D D^T,  A1 = sum D L1^T,  A2 = sum (L1 L1^T + D L2^T),
+//     A3 = sum L1 L2^T
+//   (tcgen05.mma kind::i8, five MMAs per K-step).  F = 2^30 A0 + 2^24 A1 +
+//   2^16 A2 + 2^9 A3 and S = (F + F^T)/2 is sum q q^T except the weight-1
+//   products L2 L2^T: their diagonal is added back exactly (the converters
+//   count sum L2^2 per band), and of their off-diagonal sums the mean part
+//   (sum L2_i)(sum L2_j)/N, which is what is left when the low limbs are not
+//   random residues: inputs on a coarse grid (FP16 values, integer counts)
+//   give every pixel of a band nearly the same L2.  r is placed on a grid of
+//   256 fixed-point steps for the same reason.  The cross terms matter: when
+//   outliers set the fixed-point range, typical q carry only ~15 significant
+//   bits.
 //   A ones-row at band B (q = 2^16) makes the same GEMM produce sum(q) and the
-//   pixel count.  Partial sums of all CTAs are reduced in a fixed order and
+//   pixel count.
+//   Every 32768-pixel chunk's accumulators leave TMEM as two exact INT64
+//   matrices (sum A0, and sum 2^15 A1 + 2^7 A2 + A3), so the per-CTA partials
+//   add up exactly in any order: the moments do not depend on how the pixels
+//   were split between CTAs, and come out bit-identical run to run.  They are
 //   rebuilt as raw moments in FP64 (src/linalg.cpp:81-103).
+//
+// Batches.  One launch sequence serves up to kMaxBatch frames of one element
+// type: the frames' K-blocks (128 pixels each) form one sequence that the
+// persistent GEMM splits evenly over one CTA per SM, so the pipeline runs
+// across frame boundaries and a CTA's range meets at most a few frames (each
+// meeting is a "piece" with its own partial slot).  The small steps (range
+// subsample, reduction, finalisation) each take one launch for all frames.
 //
 // Kernel roles (one CTA per SM, 22 warps):
 //   warp 0       TMA producer: 64-pixel x 128-band boxes, two per K-block,
 //                into a 4-deep ring (3 boxes in flight while one converts)
 //   warp 1       TMEM allocator + single-thread MMA issuer
-//   warps 2-17   converters: FP32 tile -> INT8 limbs L0, L1, L2 in the UMMA
-//                128-byte-swizzled K-major layout; per-band |d| maxima
-//   warps 18-21  epilogue: INT32 TMEM accumulators -> FP64 partials (once per
-//                32768-pixel chunk, i.e. once per frame at typical sizes)
+//   warps 2-17   converters: FP32 tile -> INT8 limbs D, L1, L2 in the UMMA
+//                128-byte-swizzled K-major layout; range check per element
+//   warps 18-21  epilogue: INT32 TMEM accumulators -> INT64 partials (once per
+//                32768-pixel chunk and at the end of each piece)
 // TMEM: columns [0,128) A0, [128,256) A1, [256,384) A2, [384,512) A3.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+
+#include <mutex>
 
 #include "tc.cuh"
 
@@ -62,9 +81,25 @@ constexpr int kLimbBytes = kRows * kKB;                 // 16 KB per limb tile
 constexpr uint32_t kTmemCols = 512;
 constexpr int kMaxTensorBands = kRows - 1;  // 127: room for the ones row
 constexpr int kMaxCtas = 160;
+constexpr int kMaxBatch = 64;               // frames per launch sequence
 constexpr int64_t kTensorMinPixels = 32768;
-constexpr int kQMax = (1 << 22) - (1 << 16);  // |q| bound of the FMA rounding trick
+constexpr int64_t kTensorMaxPixels = int64_t(1) << 31;  // TMA pixel coordinates are 32-bit
 constexpr int kOnesExp = 16;  // the ones row holds q = 2^16
+constexpr size_t kSlotElems = 2 * static_cast<size_t>(kRows) * kRows;  // INT64 H and Lo per piece
+
+// Fixed-point conversion by one FMA: y = x * 2^e + (kMagicQ - r * 2^e).  For
+// -2^22 - 0x8080 <= q < 2^22 - 0x8080, y = 1.5 * 2^23 + 0x8080 + q lies in
+// [2^23, 2^24), where float spacing is 1, so the FMA's rounding is rint and
+// the float's bits are 0x4B000000 + m with m = q + 0x8080 + 2^22.  The limbs
+// are m's bytes: L2 = byte0 ^ 0x80, L1 = byte1 ^ 0x80, L0 = byte2 - 64 (the
+// 0x80 offsets make the limbs balanced), and D = 2 L0 = (2 byte2) ^ 0x80.
+// Any y outside [2^23, 2^24) (q out of range, Inf, NaN) has other exponent
+// bits: OR-ing (bits ^ 0x4B000000) over all elements and testing the top nine
+// bits detects it with one instruction per element.
+constexpr float kMagicQ = 12615808.0f;        // 1.5 * 2^23 + 0x8080
+constexpr uint32_t kExpBits = 0x4B000000u;     // bits of 2^23
+constexpr uint32_t kZeroBits = 0x4B408080u;    // y for q = 0
+constexpr uint32_t kOnesBits = 0x4B418080u;    // y for q = 2^16 (the ones row)
 
 // Input stages hold one TMA box (half a K-block: 64 pixels x 128 bands).
 template <typename T>
@@ -77,7 +112,7 @@ constexpr int in_tile_bytes() {
 }
 
 struct StatsSmem {
-  size_t in_off, op_off, shift_off, scale_off, bar_off, slot_off, total;
+  size_t in_off, op_off, bar_off, slot_off, total;
 };
 
 template <typename T>
@@ -88,10 +123,6 @@ __host__ __device__ inline StatsSmem stats_smem() {
   off += static_cast<size_t>(in_stages<T>()) * in_tile_bytes<T>();
   s.op_off = off;  // 1024-aligned: in tiles are multiples of 1024
   off += static_cast<size_t>(kOpStages) * 3 * kLimbBytes;
-  s.shift_off = off;
-  off += kRows * sizeof(float);
-  s.scale_off = off;
-  off += kRows * sizeof(float);
   s.bar_off = off;
   off += (2 * 8 + 2 * kOpStages + 3) * sizeof(uint64_t);
   s.slot_off = off;
@@ -120,34 +151,96 @@ __device__ __forceinline__ float4 load4f<__half>(const __half* p) {
   return make_float4(a.x, a.y, b.x, b.y);
 }
 
-// Workspace shared by the launch sequence of one frame.
+constexpr int kShiftSplit = 16;  // blocks per band of the subsample and range passes
+
+// Per-frame state of the launch sequence.
 struct StatsState {
   float shift[HSI_MAX_BANDS + 1];     // r_b
   int scale_exp[HSI_MAX_BANDS + 1];   // e_b (ones row: kOnesExp)
-  int maxdev_bits[HSI_MAX_BANDS + 1]; // max |d_b| seen by the GEMM (float bits, >= 0)
-  int flags;                          // bit 0: a q was clamped; bit 1: the re-run is armed
+  int maxdev_bits[HSI_MAX_BANDS + 1]; // max |x_b - r_b| over the frame (float bits, >= 0), after a clamp
+  int flags;                          // bit 0: a q was out of range; bit 1: the re-run is armed
   int pad[3];
   unsigned long long l2sq[HSI_MAX_BANDS + 1];  // exact sum of L2^2 per band
-  // subsample pass (cleared by a memset before it)
-  double sub_sum[HSI_MAX_BANDS + 1];
-  double sub_cnt[HSI_MAX_BANDS + 1];
+  long long l2sum[HSI_MAX_BANDS + 1];          // exact sum of L2 per band
+  // subsample pass: per-block sums and counts (fixed slots, summed in a fixed
+  // order), range (atomics on the order-independent min / max; cleared first)
+  double sub_sum[HSI_MAX_BANDS + 1][kShiftSplit];
+  double sub_cnt[HSI_MAX_BANDS + 1][kShiftSplit];
   int sub_lo[HSI_MAX_BANDS + 1];  // float_order of the minimum
   int sub_hi[HSI_MAX_BANDS + 1];
 };
 
-struct StatsArgs {
+// One frame of a launch sequence.
+struct FrameStats {
+  const void* cube;
   int64_t pixels;
-  int bands;
+  int64_t stride;
+  int64_t kb_begin;        // first K-block of the frame in the batch's sequence
+  const float* reference;  // nullable
+  double* moments;
   StatsState* state;
-  double* partials;  // [gridDim.x][kRows][kRows] (column-major per CTA)
-  int conditional;   // 1: run only if the re-run is armed
-  int* status;
+  double* fsum;            // [kRows][kRows] F, column-major
+  long long* slots;        // nslots partial slots (H then Lo, each [kRows][kRows] column-major)
+  int bands;
+  int cta_lo;              // first CTA whose K-block range meets this frame
+  int nslots;
+  int pad;
+};
+
+struct FrameTable {
+  FrameStats f[kMaxBatch];
+  int n;
+  int max_bands;
+  int ctas;          // CTAs of the GEMM
+  int center_mean;   // reference point r: 1 = subsample mean (FP32 path), 0 = midpoint of its range
+  int64_t total_kb;  // K-blocks of all frames
+  int* status;       // nullable
+};
+
+struct GemmParams {
+  CUtensorMap maps[kMaxBatch];
+  FrameTable t;
+  int conditional;  // 1: only frames whose re-run is armed
+};
+
+__device__ __forceinline__ int64_t frame_kb(const FrameStats& F) { return div_up<int64_t>(F.pixels, kKB); }
+
+// Index of the frame holding K-block kb (the last frame starting at or before it).
+__device__ __forceinline__ int frame_of(const FrameTable& t, int64_t kb) {
+  int lo = 0, hi = t.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (t.f[mid].kb_begin <= kb) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// The pieces of CTA `cta`: its K-block range [kb0, kb1) cut at frame
+// boundaries, skipping frames whose re-run is not armed when `conditional`.
+// Every role walks the same pieces in the same order.
+struct PieceWalk {
+  const FrameTable& t;
+  int64_t kb0, kb1;
+  int conditional;
+  __device__ int first() const { return kb0 < kb1 ? frame_of(t, kb0) : t.n; }
+  __device__ bool in_range(int f) const { return f < t.n && t.f[f].kb_begin < kb1; }
+  __device__ bool skip(int f) const { return conditional && !(t.f[f].state->flags & 2); }
+  __device__ int64_t lo(int f) const { return max(kb0, t.f[f].kb_begin); }
+  __device__ int64_t hi(int f) const { return min(kb1, t.f[f].kb_begin + frame_kb(t.f[f])); }
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 1)
-    stats_gemm_kernel(const __grid_constant__ CUtensorMap cube_map, const StatsArgs args) {
-  if (args.conditional && !(args.state->flags & 2)) return;  // nothing to redo
+__global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_constant__ GemmParams p) {
+  const FrameTable& t = p.t;
+  const int64_t kb0 = t.total_kb * blockIdx.x / gridDim.x;
+  const int64_t kb1 = t.total_kb * (blockIdx.x + 1) / gridDim.x;
+  const PieceWalk walk{t, kb0, kb1, p.conditional};
+  {
+    // nothing to do (an unarmed re-run): leave before any set-up
+    bool any = false;
+    for (int f = walk.first(); walk.in_range(f); ++f) any = any || !walk.skip(f);
+    if (!any) return;
+  }
   constexpr int kInStages = in_stages<T>();
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -162,19 +255,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* mma_done = acc_empty + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.slot_off);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.slot_off + 8);
-  int* clamp_flag = reinterpret_cast<int*>(smem + L.slot_off + 12);
-  float* shift = reinterpret_cast<float*>(smem + L.shift_off);
-  float* scale = reinterpret_cast<float*>(smem + L.scale_off);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t P = args.pixels;
-  const int B = args.bands;
-  const int64_t nkb = div_up<int64_t>(P, kKB);
-  const int64_t kb0 = nkb * blockIdx.x / gridDim.x;
-  const int64_t kb1 = nkb * (blockIdx.x + 1) / gridDim.x;
-  const int n = static_cast<int>(kb1 - kb0);
-  const int nchunks = (n + kChunkKB - 1) / kChunkKB;
-
   if (threadIdx.x == 0) {
     for (int s = 0; s < kInStages; ++s) {
       mbar_init(&in_full[s], 1);
@@ -188,12 +270,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(acc_empty, kEpiWarps);
     mbar_init(mma_done, 1);
     *abort_flag = 0;
-    *clamp_flag = 0;
     fence_barrier_init();
-  }
-  for (int i = threadIdx.x; i < kRows; i += blockDim.x) {
-    shift[i] = args.state->shift[i];
-    scale[i] = ldexpf(1.0f, args.state->scale_exp[i]);
   }
   if (warp == kWarpMma) tmem_alloc(tmem_slot, kTmemCols);
   tc_fence_before();
@@ -203,21 +280,30 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == kWarpTma) {
     if (lane == 0) {
-      prefetch_tensormap(&cube_map);
-      uint32_t pending = 0, parity = 0;
-      for (int i = 0; i < 2 * n; ++i) {
-        const int s = i % kInStages;
-        const uint32_t ph = (i / kInStages) & 1u;
-        if (*abort_flag || !mbar_wait(&in_empty[s], ph ^ 1u)) {
-          record_error(args.status, HSI_E_TIMEOUT);
-          *abort_flag = 1;
-          break;
+      uint32_t box = 0, pending = 0, parity = 0;
+      bool ok = true;
+      for (int f = walk.first(); ok && walk.in_range(f); ++f) {
+        if (walk.skip(f)) continue;
+        const CUtensorMap* map = &p.maps[f];
+        prefetch_tensormap(map);
+        const int64_t kbf = t.f[f].kb_begin;
+        for (int64_t kb = walk.lo(f); kb < walk.hi(f) && ok; ++kb) {
+          for (int half = 0; half < 2; ++half, ++box) {
+            const int s = box % kInStages;
+            const uint32_t ph = (box / kInStages) & 1u;
+            if (*abort_flag || !mbar_wait(&in_empty[s], ph ^ 1u)) {
+              record_error(t.status, HSI_E_TIMEOUT);
+              *abort_flag = 1;
+              ok = false;
+              break;
+            }
+            unsigned char* dst = smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>();
+            mbar_arrive_expect_tx(&in_full[s], in_tile_bytes<T>());
+            tma_load_2d(dst, map, static_cast<int>((kb - kbf) * kKB + half * kBoxPx), 0, &in_full[s]);
+            pending |= 1u << s;
+            parity = (parity & ~(1u << s)) | (ph << s);
+          }
         }
-        unsigned char* dst = smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>();
-        mbar_arrive_expect_tx(&in_full[s], in_tile_bytes<T>());
-        tma_load_2d(dst, &cube_map, static_cast<int>(kb0 * kKB + static_cast<int64_t>(i) * kBoxPx), 0, &in_full[s]);
-        pending |= 1u << s;
-        parity = (parity & ~(1u << s)) | (ph << s);
       }
       for (int s = 0; s < kInStages; ++s)
         if ((pending >> s) & 1u) mbar_wait(&in_full[s], (parity >> s) & 1u);
@@ -225,49 +311,56 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == kWarpMma) {
     if (lane == 0) {
       const uint32_t idesc = idesc_s8_s32(kRows, kRows);
-      bool issued = false;
-      for (int i = 0; i < n && !*abort_flag; ++i) {
-        const int chunk = i / kChunkKB, j = i % kChunkKB;
-        if (j == 0) {
-          if (!mbar_wait(acc_empty, (chunk & 1u) ^ 1u)) {
-            record_error(args.status, HSI_E_TIMEOUT);
+      uint32_t i = 0, chunk = 0;  // K-blocks and chunks issued so far
+      bool ok = true;
+      for (int f = walk.first(); ok && walk.in_range(f); ++f) {
+        if (walk.skip(f)) continue;
+        const int64_t lo = walk.lo(f), hi = walk.hi(f);
+        for (int64_t kb = lo; kb < hi; ++kb, ++i) {
+          const int j = static_cast<int>((kb - lo) % kChunkKB);
+          if (j == 0) {
+            if (*abort_flag || !mbar_wait(acc_empty, (chunk & 1u) ^ 1u)) {
+              record_error(t.status, HSI_E_TIMEOUT);
+              *abort_flag = 1;
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+          }
+          const int so = i % kOpStages;
+          if (!mbar_wait(&op_full[so], (i / kOpStages) & 1u)) {
+            record_error(t.status, HSI_E_TIMEOUT);
             *abort_flag = 1;
+            ok = false;
             break;
           }
           tc_fence_after();
-        }
-        const int so = i % kOpStages;
-        if (!mbar_wait(&op_full[so], (i / kOpStages) & 1u)) {
-          record_error(args.status, HSI_E_TIMEOUT);
-          *abort_flag = 1;
-          break;
-        }
-        tc_fence_after();
-        unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kLimbBytes;
-        const uint64_t d0 = smem_desc_sw128(op);
-        const uint64_t d1 = smem_desc_sw128(op + kLimbBytes);
-        const uint64_t d2 = smem_desc_sw128(op + 2 * kLimbBytes);
+          unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kLimbBytes;
+          const uint64_t dd = smem_desc_sw128(op);
+          const uint64_t d1 = smem_desc_sw128(op + kLimbBytes);
+          const uint64_t d2 = smem_desc_sw128(op + 2 * kLimbBytes);
 #pragma unroll
-        for (int k = 0; k < kKB / 32; ++k) {
-          const uint64_t adv = static_cast<uint64_t>(k * 2);  // 32 bytes of K, in 16-byte units
-          const uint32_t acc = (j > 0 || k > 0) ? 1u : 0u;
-          umma_i8(tmem + 0, d0 + adv, d0 + adv, idesc, acc);
-          umma_i8(tmem + 128, d0 + adv, d1 + adv, idesc, acc);
-          umma_i8(tmem + 256, d1 + adv, d1 + adv, idesc, acc);
-          umma_i8(tmem + 256, d0 + adv, d2 + adv, idesc, 1u);
-          umma_i8(tmem + 256, d0 + adv, d2 + adv, idesc, 1u);
-          umma_i8(tmem + 384, d1 + adv, d2 + adv, idesc, acc);
-          umma_i8(tmem + 384, d1 + adv, d2 + adv, idesc, 1u);
+          for (int k = 0; k < kKB / 32; ++k) {
+            const uint64_t adv = static_cast<uint64_t>(k * 2);  // 32 bytes of K, in 16-byte units
+            const uint32_t acc = (j > 0 || k > 0) ? 1u : 0u;
+            umma_i8(tmem + 0, dd + adv, dd + adv, idesc, acc);    // A0 = D D^T
+            umma_i8(tmem + 128, dd + adv, d1 + adv, idesc, acc);  // A1 = D L1^T
+            umma_i8(tmem + 256, d1 + adv, d1 + adv, idesc, acc);  // A2 = L1 L1^T
+            umma_i8(tmem + 256, dd + adv, d2 + adv, idesc, 1u);   //    + D L2^T
+            umma_i8(tmem + 384, d1 + adv, d2 + adv, idesc, acc);  // A3 = L1 L2^T
+          }
+          umma_commit(&op_empty[so]);
+          if (j == kChunkKB - 1 || kb == hi - 1) {
+            umma_commit(acc_full);
+            ++chunk;
+          }
         }
-        umma_commit(&op_empty[so]);
-        if (j == kChunkKB - 1 || i == n - 1) umma_commit(acc_full);
-        issued = true;
       }
       // TMEM is freed at the end of the kernel: make sure no MMA of this
       // thread is still running by then (bounded wait).
-      if (issued) {
+      if (i > 0) {
         umma_commit(mma_done);
-        if (!mbar_wait(mma_done, 0)) record_error(args.status, HSI_E_TIMEOUT);
+        if (!mbar_wait(mma_done, 0)) record_error(t.status, HSI_E_TIMEOUT);
       }
     }
   } else if (warp < kWarpEpi0) {
@@ -276,140 +369,183 @@ __global__ void __launch_bounds__(kThreads, 1)
     // pairs (b, b+4) -- lanes 0-15 the first band, 16-31 the second, 4 pixels
     // per lane -- so one store instruction covers two rows whose swizzled
     // chunks never share a bank.
-    // q = rint((x - r) 2^e) comes out of one FMA: adding 1.5*2^23 leaves
-    // rint(q) in the low mantissa bits (|q| < 2^22), and w = q + 0x8080 has
-    // the balanced limbs as its bytes (low two XOR 0x80, third as is).
     const int cw = warp - kWarpConv0;
     constexpr int kSlots = kRows / 2 / kConvWarps;  // 4 band pairs per warp
-    constexpr float kMagic = 12582912.0f;          // 1.5 * 2^23
     const int sub = lane >> 4, lp = (lane & 15) * 4;  // which band of the pair; pixel in the box
-    int band[kSlots];
-    float sc[kSlots], off[kSlots], xlo[kSlots], xhi[kSlots];
-    int l2sq[kSlots];
-#pragma unroll
-    for (int t = 0; t < kSlots; ++t) {
-      const int pair = cw + kConvWarps * t;          // 0..63
-      const int b = (pair >> 2) * 8 + (pair & 3) + 4 * sub;
-      band[t] = b;
-      sc[t] = scale[b];
-      off[t] = kMagic - shift[b] * scale[b];  // exact: r sits on the 2^-e grid
-      xlo[t] = INFINITY;
-      xhi[t] = -INFINITY;
-      l2sq[t] = 0;
-    }
-    const int wbias = __float_as_int(kMagic) - 0x8080;
+    // slot t2 holds band pair cw + 16 t2, i.e. band band0 + 32 t2 (four 8-row
+    // swizzle atoms further down: byte offset o0 + 4096 t2); the second half of
+    // a K-block sits 64 bytes along, i.e. four 16-byte chunks, which the swizzle
+    // maps to o ^ 64
+    const int band0 = (cw >> 2) * 8 + (cw & 3) + 4 * sub;
+    const uint32_t o0 = sw128_byte(band0, lp);
+    uint32_t box = 0, i = 0;
     bool aborted = false;
-    for (int j = 0; j < 2 * n; ++j) {
-      const int s = j % kInStages, i = j >> 1, half = j & 1, so = i % kOpStages;
-      if (!aborted && (!mbar_wait(&in_full[s], (j / kInStages) & 1u) ||
-                       (half == 0 && !mbar_wait(&op_empty[so], ((i / kOpStages) & 1u) ^ 1u)))) {
-        record_error(args.status, HSI_E_TIMEOUT);
-        *abort_flag = 1;
-        aborted = true;
-      }
-      if (aborted) break;
-      const T* in = reinterpret_cast<const T*>(smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>());
-      unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kLimbBytes;
-      const int64_t gp = (kb0 + i) * kKB + half * kBoxPx + lp;
-      const int nvalid = gp >= P ? 0 : (P - gp >= 4 ? 4 : static_cast<int>(P - gp));
+    for (int f = walk.first(); !aborted && walk.in_range(f); ++f) {
+      if (walk.skip(f)) continue;
+      const FrameStats& F = t.f[f];
+      const int B = F.bands;
+      const int64_t P = F.pixels;
+      float sc[kSlots], off[kSlots];
 #pragma unroll
-      for (int t = 0; t < kSlots; ++t) {
-        const int b = band[t];
-        int w[4] = {0x8080, 0x8080, 0x8080, 0x8080};  // q = 0
+      for (int t2 = 0; t2 < kSlots; ++t2) {
+        const int b = band0 + 32 * t2;
+        sc[t2] = 0.0f;
+        off[t2] = 0.0f;
         if (b < B) {
-          const float4 x = load4f<T>(in + b * kBoxPx + lp);
-          const float xv[4] = {x.x, x.y, x.z, x.w};
-          // fully unrolled with a predicate: a loop bounded by nvalid would
-          // index w[] dynamically and move it to local memory
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            if (e < nvalid) {
-              xlo[t] = fminf(xlo[t], xv[e]);
-              xhi[t] = fmaxf(xhi[t], xv[e]);
-              w[e] = __float_as_int(fmaf(xv[e], sc[t], off[t])) - wbias;
-            }
-          }
-        } else if (b == B) {
-#pragma unroll
-          for (int e = 0; e < 4; ++e) w[e] = e < nvalid ? (1 << kOnesExp) + 0x8080 : 0x8080;
+          const float s = ldexpf(1.0f, F.state->scale_exp[b]);
+          sc[t2] = s;
+          off[t2] = kMagicQ - F.state->shift[b] * s;  // exact when r * 2^e stays below 2^23
         }
-        const uint32_t p01 = __byte_perm(w[0], w[1], 0x5140), p23 = __byte_perm(w[2], w[3], 0x5140);
-        const uint32_t h01 = __byte_perm(w[0], w[1], 0x7362), h23 = __byte_perm(w[2], w[3], 0x7362);
-        const uint32_t l2 = __byte_perm(p01, p23, 0x5410) ^ 0x80808080u;
-        const uint32_t l1 = __byte_perm(p01, p23, 0x7632) ^ 0x80808080u;
-        const uint32_t l0 = __byte_perm(h01, h23, 0x5410);
-        l2sq[t] = __dp4a(static_cast<int>(l2), static_cast<int>(l2), l2sq[t]);
-        const uint32_t o = sw128_byte(b, half * kBoxPx + lp);
-        *reinterpret_cast<uint32_t*>(op + o) = l0;
-        *reinterpret_cast<uint32_t*>(op + kLimbBytes + o) = l1;
-        *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + o) = l2;
       }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&in_empty[s]);
-      if (half == 1) {
-        fence_proxy_async_smem();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&op_full[so]);
-      }
-    }
-    // per band: |x - r| range (for the re-run and for the whitening pass), the
-    // clamp check, and the exact sum of L2^2 (reduced over the 16 lanes that
-    // share the band)
-    bool clamped = false;
+      uint32_t chk = 0u;
+      // sums of L2^2 and of L2 per lane in 32 bits (at most 64 * 8 * 2^14 =
+      // 2^23 between flushes), added to the frame's 64-bit counters every 64
+      // K-blocks
+      unsigned int l2sq[kSlots] = {0u, 0u, 0u, 0u};
+      int l2s[kSlots] = {0, 0, 0, 0};
+      auto flush_l2 = [&]() {
 #pragma unroll
-    for (int t = 0; t < kSlots; ++t) {
-      float lo = xlo[t], hi = xhi[t];
-      unsigned long long sq = static_cast<unsigned int>(l2sq[t]);
+        for (int t2 = 0; t2 < kSlots; ++t2) {
+          unsigned long long sq = l2sq[t2];
+          long long sm = l2s[t2];
 #pragma unroll
-      for (int o = 8; o > 0; o >>= 1) {
-        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-        sq += __shfl_xor_sync(0xffffffffu, sq, o);
+          for (int o = 8; o > 0; o >>= 1) {
+            sq += __shfl_xor_sync(0xffffffffu, sq, o);
+            sm += __shfl_xor_sync(0xffffffffu, sm, o);
+          }
+          const int b = band0 + 32 * t2;
+          if ((lane & 15) == 0 && b < B) {
+            if (sq != 0ull) atomicAdd(&F.state->l2sq[b], sq);
+            if (sm != 0ll)
+              atomicAdd(reinterpret_cast<unsigned long long*>(&F.state->l2sum[b]),
+                        static_cast<unsigned long long>(sm));  // two's complement: adds mod 2^64
+          }
+          l2sq[t2] = 0u;
+          l2s[t2] = 0;
+        }
+      };
+      int since_flush = 0;
+      for (int64_t kb = walk.lo(f); kb < walk.hi(f) && !aborted; ++kb, ++i) {
+        const int so = i % kOpStages;
+        unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kLimbBytes;
+#pragma unroll
+        for (int half = 0; half < 2; ++half, ++box) {
+          const int s = box % kInStages;
+          if (!mbar_wait(&in_full[s], (box / kInStages) & 1u) ||
+              (half == 0 && !mbar_wait(&op_empty[so], ((i / kOpStages) & 1u) ^ 1u))) {
+            record_error(t.status, HSI_E_TIMEOUT);
+            *abort_flag = 1;
+            aborted = true;
+            break;
+          }
+          const T* in = reinterpret_cast<const T*>(smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>());
+          const int64_t gp = (kb - F.kb_begin) * kKB + half * kBoxPx + lp;
+          const int nvalid = gp >= P ? 0 : (P - gp >= 4 ? 4 : static_cast<int>(P - gp));
+#pragma unroll
+          for (int t2 = 0; t2 < kSlots; ++t2) {
+            const int b = band0 + 32 * t2;
+            uint32_t y[4] = {kZeroBits, kZeroBits, kZeroBits, kZeroBits};
+            if (b < B) {
+              const float4 x = load4f<T>(in + b * kBoxPx + lp);
+              const float xv[4] = {x.x, x.y, x.z, x.w};
+              // fully unrolled with a predicate: a loop bounded by nvalid would
+              // index y[] dynamically and move it to local memory
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                if (e < nvalid) {
+                  y[e] = __float_as_uint(fmaf(xv[e], sc[t2], off[t2]));
+                  chk |= y[e] ^ kExpBits;
+                }
+              }
+            } else if (b == B) {
+#pragma unroll
+              for (int e = 0; e < 4; ++e) y[e] = e < nvalid ? kOnesBits : kZeroBits;
+            }
+            const uint32_t p01 = __byte_perm(y[0], y[1], 0x5140), p23 = __byte_perm(y[2], y[3], 0x5140);
+            const uint32_t h01 = __byte_perm(y[0], y[1], 0x7362), h23 = __byte_perm(y[2], y[3], 0x7362);
+            const uint32_t l2 = __byte_perm(p01, p23, 0x5410) ^ 0x80808080u;
+            const uint32_t l1 = __byte_perm(p01, p23, 0x7632) ^ 0x80808080u;
+            // byte2 <= 127 in range, so the shift carries nothing across bytes
+            const uint32_t dl = (__byte_perm(h01, h23, 0x5410) << 1) ^ 0x80808080u;
+            // signed bytes: the limbs are two's-complement INT8
+            l2sq[t2] = static_cast<unsigned int>(
+                __dp4a(static_cast<int>(l2), static_cast<int>(l2), static_cast<int>(l2sq[t2])));
+            l2s[t2] = __dp4a(static_cast<int>(l2), 0x01010101, l2s[t2]);
+            const uint32_t o = (o0 + 4096u * t2) ^ (half ? 64u : 0u);
+            *reinterpret_cast<uint32_t*>(op + o) = dl;
+            *reinterpret_cast<uint32_t*>(op + kLimbBytes + o) = l1;
+            *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + o) = l2;
+          }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&in_empty[s]);
+          if (half == 1) {
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&op_full[so]);
+          }
+        }
+        if (++since_flush == 64) {
+          flush_l2();
+          since_flush = 0;
+        }
       }
-      const int b = band[t];
-      const float r = shift[b];
-      const float m = hi >= lo ? fmaxf(hi - r, r - lo) : 0.0f;
-      if (b < B && !(m * sc[t] <= static_cast<float>(kQMax))) clamped = true;
-      if ((lane & 15) == 0 && b < B) {
-        atomicMax(&args.state->maxdev_bits[b], __float_as_int(m));
-        atomicAdd(&args.state->l2sq[b], sq);
-      }
+      // end of the piece: the remaining L2^2 sums and the range check
+      flush_l2();
+      if (__any_sync(0xffffffffu, (chk >> 23) != 0u) && lane == 0) atomicOr(&F.state->flags, 1);
     }
-    if (__any_sync(0xffffffffu, clamped) && lane == 0) atomicOr(&args.state->flags, 1);
   } else {
     // ---------------- epilogue ----------------
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int row = q * 32 + lane;
     const uint32_t trow = tmem + (static_cast<uint32_t>(q * 32) << 16);
-    double* out = args.partials + static_cast<size_t>(blockIdx.x) * kRows * kRows;
-    for (int chunk = 0; chunk < nchunks; ++chunk) {
-      if (!mbar_wait(acc_full, chunk & 1u)) {
-        record_error(args.status, HSI_E_TIMEOUT);
-        *abort_flag = 1;
-        break;
-      }
-      tc_fence_after();
-#pragma unroll 1
-      for (int cb = 0; cb < kRows / 16; ++cb) {
-        uint32_t a0[16], a1[16], a2[16], a3[16];
-        tmem_ld16(trow + 0 + 16 * cb, a0);
-        tmem_ld16(trow + 128 + 16 * cb, a1);
-        tmem_ld16(trow + 256 + 16 * cb, a2);
-        tmem_ld16(trow + 384 + 16 * cb, a3);
-        tmem_wait_ld();
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const double f = ldexp(static_cast<double>(static_cast<int>(a0[j])), 32) +
-                           ldexp(static_cast<double>(static_cast<int>(a1[j])), 25) +
-                           ldexp(static_cast<double>(static_cast<int>(a2[j])), 16) +
-                           ldexp(static_cast<double>(static_cast<int>(a3[j])), 8);
-          double* dst = out + static_cast<size_t>(16 * cb + j) * kRows + row;  // column-major
-          *dst = chunk == 0 ? f : *dst + f;
+    uint32_t chunk = 0;
+    bool ok = true;
+    for (int f = walk.first(); ok && walk.in_range(f); ++f) {
+      if (walk.skip(f)) continue;
+      const FrameStats& F = t.f[f];
+      long long* outH = F.slots + static_cast<size_t>(blockIdx.x - F.cta_lo) * kSlotElems;
+      long long* outL = outH + kRows * kRows;
+      const int64_t nkb = walk.hi(f) - walk.lo(f);
+      const int nch = static_cast<int>(div_up<int64_t>(nkb, kChunkKB));
+      for (int c = 0; c < nch; ++c, ++chunk) {
+        if (*abort_flag || !mbar_wait(acc_full, chunk & 1u)) {
+          record_error(t.status, HSI_E_TIMEOUT);
+          *abort_flag = 1;
+          ok = false;
+          break;
         }
+        tc_fence_after();
+#pragma unroll 1
+        for (int cb = 0; cb < kRows / 16; ++cb) {
+          const size_t e0 = static_cast<size_t>(16 * cb) * kRows + row;  // column-major
+          {
+            uint32_t a0[16];
+            tmem_ld16(trow + 0 + 16 * cb, a0);
+            tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              long long* d = outH + e0 + static_cast<size_t>(j) * kRows;
+              *d = (c == 0 ? 0ll : *d) + static_cast<int>(a0[j]);
+            }
+          }
+          uint32_t a1[16], a2[16], a3[16];
+          tmem_ld16(trow + 128 + 16 * cb, a1);
+          tmem_ld16(trow + 256 + 16 * cb, a2);
+          tmem_ld16(trow + 384 + 16 * cb, a3);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const long long l = (static_cast<long long>(static_cast<int>(a1[j])) << 15) +
+                                (static_cast<long long>(static_cast<int>(a2[j])) << 7) +
+                                static_cast<long long>(static_cast<int>(a3[j]));
+            long long* d = outL + e0 + static_cast<size_t>(j) * kRows;
+            *d = (c == 0 ? 0ll : *d) + l;
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acc_empty);
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(acc_empty);
     }
   }
   tc_fence_before();
@@ -423,8 +559,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // ---------------------------------------------------------------------------
 // Reference point and fixed-point scale per band from a regular subsample
-// (every 16th run of 64 pixels on large frames): r = subsample mean, e such
-// that the subsample's largest |x - r| maps to 2^20 (4x headroom below 2^22).
+// (every 16th run of 64 pixels on large frames): r = the midpoint of the
+// subsample's range (which minimises its largest |x - r|, and, being built
+// from a minimum and a maximum, does not depend on the order the blocks
+// finish in), e such that that largest |x - r| maps to 2^20 (4x headroom
+// below 2^22).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int scale_exp_for(float maxdev) {
   if (!(maxdev > 0.0f)) return 20;
@@ -442,45 +581,20 @@ __device__ __forceinline__ int float_order(float v) {
 }
 __device__ __forceinline__ float order_float(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
 
-constexpr int kShiftSplit = 16;  // blocks per band of the subsample pass
-
-__global__ void shift_init_kernel(StatsState* st) {
+// One block per frame.
+__global__ void shift_init_kernel(const __grid_constant__ FrameTable t) {
+  StatsState* st = t.f[blockIdx.x].state;
   for (int b = threadIdx.x; b <= HSI_MAX_BANDS; b += blockDim.x) {
-    st->sub_sum[b] = 0.0;
-    st->sub_cnt[b] = 0.0;
     st->sub_lo[b] = 0x7fffffff;
     st->sub_hi[b] = static_cast<int>(0x80000000u);
   }
 }
 
-// Subsample statistics, spread over (bands x kShiftSplit) blocks: runs of 64
-// pixels, every 16th run on large frames; partial sums land in the state with
-// atomics (the state is cleared by a memset first).
-template <typename T>
-__global__ void __launch_bounds__(256) shift_partial_kernel(const T* __restrict__ cube, int64_t pixels,
-                                                            int64_t stride, int bands, StatsState* st) {
-  const int b = blockIdx.x;
-  if (b >= bands) return;
+// Block-wide sum / count (into this block's slot) and min / max (folded into
+// the frame's state with atomics).
+__device__ void fold_subsample(double sum, double cnt, float lo, float hi, StatsState* st, int b) {
   __shared__ double s_sum[8], s_cnt[8];
   __shared__ int s_lo[8], s_hi[8];
-  const T* plane = cube + static_cast<int64_t>(b) * stride;
-  const int64_t runs = div_up<int64_t>(pixels, 64);
-  const int64_t step = runs > 4096 ? 16 : 1;
-  const int64_t sampled = div_up<int64_t>(runs, step);
-  const int64_t r0 = sampled * blockIdx.y / kShiftSplit, r1 = sampled * (blockIdx.y + 1) / kShiftSplit;
-  double sum = 0.0, cnt = 0.0;
-  float lo = INFINITY, hi = -INFINITY;
-#pragma unroll 4
-  for (int64_t run = r0 + threadIdx.x / 64; run < r1; run += blockDim.x / 64) {
-    const int64_t p = run * step * 64 + (threadIdx.x & 63);
-    if (p < pixels) {
-      const float v = static_cast<float>(plane[p]);
-      sum += static_cast<double>(v);
-      cnt += 1.0;
-      lo = fminf(lo, v);
-      hi = fmaxf(hi, v);
-    }
-  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -497,31 +611,67 @@ __global__ void __launch_bounds__(256) shift_partial_kernel(const T* __restrict_
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double ts = 0.0, tc = 0.0;
+    double ts = s_sum[0], tc = s_cnt[0];
     int tl = s_lo[0], th = s_hi[0];
-    for (int w = 0; w < 8; ++w) {
+    for (int w = 1; w < 8; ++w) {
       ts += s_sum[w];
       tc += s_cnt[w];
       tl = min(tl, s_lo[w]);
       th = max(th, s_hi[w]);
     }
-    if (tc > 0.0) {
-      atomicAdd(&st->sub_sum[b], ts);
-      atomicAdd(&st->sub_cnt[b], tc);
+    st->sub_sum[b][blockIdx.y] = ts;
+    st->sub_cnt[b][blockIdx.y] = tc;
+    if (tl <= th) {  // the block saw a value other than NaN
       atomicMin(&st->sub_lo[b], tl);
       atomicMax(&st->sub_hi[b], th);
     }
   }
 }
 
-// r = subsample mean (or the caller's reference), e such that the subsample's
-// largest |x - r| maps to 2^20 (4x headroom below 2^22), r snapped to the
-// 2^-e grid so that inputs on that grid (FP16 cubes) convert exactly.
-__global__ void __launch_bounds__(256) shift_finalize_kernel(int bands, const float* __restrict__ given,
-                                                             StatsState* st) {
+// Subsample statistics, grid (bands, kShiftSplit, frames): runs of 64
+// pixels, every 16th run on large frames.
+template <typename T>
+__global__ void __launch_bounds__(256) shift_partial_kernel(const __grid_constant__ FrameTable t) {
+  const FrameStats& F = t.f[blockIdx.z];
+  const int b = blockIdx.x;
+  if (b >= F.bands) return;
+  const T* plane = static_cast<const T*>(F.cube) + static_cast<int64_t>(b) * F.stride;
+  const int64_t pixels = F.pixels;
+  const int64_t runs = div_up<int64_t>(pixels, 64);
+  const int64_t step = runs > 4096 ? 16 : 1;
+  const int64_t sampled = div_up<int64_t>(runs, step);
+  const int64_t r0 = sampled * blockIdx.y / kShiftSplit, r1 = sampled * (blockIdx.y + 1) / kShiftSplit;
+  double sum = 0.0, cnt = 0.0;
+  float lo = INFINITY, hi = -INFINITY;
+#pragma unroll 4
+  for (int64_t run = r0 + threadIdx.x / 64; run < r1; run += blockDim.x / 64) {
+    const int64_t px = run * step * 64 + (threadIdx.x & 63);
+    if (px < pixels) {
+      const float v = static_cast<float>(plane[px]);
+      if (t.center_mean) {
+        sum += static_cast<double>(v);
+        cnt += 1.0;
+      }
+      lo = fminf(lo, v);
+      hi = fmaxf(hi, v);
+    }
+  }
+  fold_subsample(sum, cnt, lo, hi, F.state, b);
+}
+
+// One block per frame: r = the caller's reference, else the midpoint of the
+// subsample's range (tensor path) or its mean (FP32 path, whose rounding
+// grows with |mean - r|), e such that the subsample's largest |x - r| maps to
+// 2^20 (4x headroom below 2^22), r snapped to the 2^-e grid so that inputs on
+// that grid (FP16 cubes) convert exactly.
+__global__ void __launch_bounds__(256) shift_finalize_kernel(const __grid_constant__ FrameTable t) {
+  const FrameStats& F = t.f[blockIdx.x];
+  StatsState* st = F.state;
+  const int bands = F.bands;
   for (int b = threadIdx.x; b <= HSI_MAX_BANDS; b += blockDim.x) {
     st->maxdev_bits[b] = 0;
     st->l2sq[b] = 0ull;
+    st->l2sum[b] = 0ll;
     if (b > bands) {
       st->shift[b] = 0.0f;
       st->scale_exp[b] = 0;
@@ -532,65 +682,115 @@ __global__ void __launch_bounds__(256) shift_finalize_kernel(int bands, const fl
       st->scale_exp[b] = kOnesExp;
       continue;
     }
-    const double c = st->sub_cnt[b];
-    float r = given ? given[b] : (c > 0.0 ? static_cast<float>(st->sub_sum[b] / c) : 0.0f);
-    const float lo = c > 0.0 ? order_float(st->sub_lo[b]) : r, hi = c > 0.0 ? order_float(st->sub_hi[b]) : r;
+    const bool seen = st->sub_lo[b] <= st->sub_hi[b];
+    const float slo = order_float(st->sub_lo[b]), shi = order_float(st->sub_hi[b]);
+    float r = 0.0f;
+    if (F.reference) {
+      r = F.reference[b];
+    } else if (t.center_mean) {
+      double sum = 0.0, cnt = 0.0;
+      for (int k = 0; k < kShiftSplit; ++k) {
+        sum += st->sub_sum[b][k];
+        cnt += st->sub_cnt[b][k];
+      }
+      r = cnt > 0.0 ? static_cast<float>(sum / cnt) : 0.0f;
+    } else if (seen) {
+      r = 0.5f * slo + 0.5f * shi;
+    }
+    const float lo = seen ? slo : r, hi = seen ? shi : r;
     const int e = scale_exp_for(fmaxf(fabsf(hi - r), fabsf(lo - r)) * 1.0000001f);
-    r = ldexpf(rintf(ldexpf(r, e)), -e);
+    // FP32 path: r on the 2^-e grid, so that inputs on that grid (FP16
+    // cubes) convert exactly.  Tensor path: r on the 256x coarser grid, so
+    // that r * 2^e is a multiple of 256 and adds nothing to the low limb
+    // (inputs on a grid of 256 steps -- integer counts, most FP16 values --
+    // then have L2 = 0 and exact moments).
+    const int g = t.center_mean ? e : e - 8;
+    r = ldexpf(rintf(ldexpf(r, g)), -g);
     st->shift[b] = r;
     st->scale_exp[b] = e;
   }
   if (threadIdx.x == 0) st->flags = 0;
 }
 
-// After the first GEMM: if a value was clamped, take the range the GEMM
-// actually saw and arm the conditional re-run; otherwise leave it disarmed.
-__global__ void rescale_kernel(int bands, StatsState* st) {
+// After the first GEMM, for frames where a value fell out of range only:
+// max |x - r| per band over the whole frame.  Work items are (frame, band,
+// slice of 1/kShiftSplit of the pixels), strided over a small grid, so that
+// the usual case -- no frame out of range -- costs one flag test per item.
+template <typename T>
+__global__ void __launch_bounds__(256) range_kernel(const __grid_constant__ FrameTable t) {
+  const int per_frame = t.max_bands * kShiftSplit;
+  for (int item = blockIdx.x; item < t.n * per_frame; item += gridDim.x) {
+    const FrameStats& F = t.f[item / per_frame];
+    const int b = (item % per_frame) / kShiftSplit, split = item % kShiftSplit;
+    if (b >= F.bands || !(F.state->flags & 1)) continue;
+    const T* plane = static_cast<const T*>(F.cube) + static_cast<int64_t>(b) * F.stride;
+    const int64_t per = div_up<int64_t>(F.pixels, kShiftSplit);
+    const int64_t p0 = per * split, p1 = min(F.pixels, p0 + per);
+    float lo = INFINITY, hi = -INFINITY;
+    for (int64_t px = p0 + threadIdx.x; px < p1; px += blockDim.x) {
+      const float v = static_cast<float>(plane[px]);
+      lo = fminf(lo, v);
+      hi = fmaxf(hi, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0 && hi >= lo) {
+      const float r = F.state->shift[b];
+      atomicMax(&F.state->maxdev_bits[b], __float_as_int(fmaxf(hi - r, r - lo)));
+    }
+  }
+}
+
+// One block per frame: if a value was out of range, take the range of the
+// whole frame and arm the conditional re-run; otherwise leave it disarmed.
+__global__ void rescale_kernel(const __grid_constant__ FrameTable t) {
+  StatsState* st = t.f[blockIdx.x].state;
   if (!(st->flags & 1)) return;
-  for (int b = threadIdx.x; b < bands; b += blockDim.x) {
+  for (int b = threadIdx.x; b < t.f[blockIdx.x].bands; b += blockDim.x) {
     const float dev = __int_as_float(st->maxdev_bits[b]);
     const int e = scale_exp_for(dev * 1.0000001f) + 1;  // observed max -> below 2^21
     st->scale_exp[b] = e;
-    // keep r on the (coarser) new grid so r * 2^e stays an exact integer
-    st->shift[b] = ldexpf(rintf(ldexpf(st->shift[b], e)), -e);
+    // keep r on the 256x coarser grid of the new scale (as shift_finalize)
+    st->shift[b] = ldexpf(rintf(ldexpf(st->shift[b], e - 8)), -(e - 8));
     st->l2sq[b] = 0ull;  // recounted by the re-run
+    st->l2sum[b] = 0ll;
   }
   __syncthreads();
   if (threadIdx.x == 0) st->flags = 2;
 }
 
-// Sum the CTAs' partial matrices in a fixed order: block = 32 entries, each of
-// 8 warps sums a slice of CTAs, then the slices are added in warp order.
-__global__ void __launch_bounds__(256) stats_reduce_kernel(const double* __restrict__ partials, int ctas,
-                                                          double* __restrict__ fsum) {
-  __shared__ double s[8][32];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int e = blockIdx.x * 32 + lane;  // entry index in [0, 128*128)
-  double acc = 0.0;
-  const int c0 = ctas * warp / 8, c1 = ctas * (warp + 1) / 8;
-  for (int c = c0; c < c1; ++c) acc += partials[static_cast<size_t>(c) * kRows * kRows + e];
-  s[warp][lane] = acc;
-  __syncthreads();
-  if (warp == 0) {
-    double t = 0.0;
-    for (int w = 0; w < 8; ++w) t += s[w][lane];
-    fsum[e] = t;
+// Sum the pieces' INT64 partials of each frame (exact, so the order is free)
+// and form F = 2^30 H + 2^9 Lo in FP64.  Grid (kRows * kRows / 256, frames).
+__global__ void __launch_bounds__(256) stats_reduce_kernel(const __grid_constant__ FrameTable t) {
+  const FrameStats& F = t.f[blockIdx.y];
+  const int e = blockIdx.x * 256 + threadIdx.x;  // entry in [0, 128*128)
+  long long h = 0, l = 0;
+  for (int s = 0; s < F.nslots; ++s) {
+    const long long* slot = F.slots + static_cast<size_t>(s) * kSlotElems;
+    h += slot[e];
+    l += slot[kRows * kRows + e];
   }
+  F.fsum[e] = ldexp(static_cast<double>(h), 30) + ldexp(static_cast<double>(l), 9);
 }
 
 // S = (F + F^T)/2, unscaled -> shifted sums (S1, S2, N) -> raw moments in FP64
 // (moments_from_shifted, src/linalg.cpp:81-103).  fsum is column-major:
 // fsum[col * 128 + row] = F[row][col].  Output: sum[B], outer[B*B] (full,
-// symmetric), count.
-__global__ void __launch_bounds__(128) stats_finalize_kernel(const double* __restrict__ fsum,
-                                                            const StatsState* __restrict__ st, int bands,
-                                                            double* __restrict__ moments) {
-  // one block per row i of the output; every block rebuilds the first moments
+// symmetric), count.  Grid (max bands, frames): block (i, f) writes row i.
+__global__ void __launch_bounds__(128) stats_finalize_kernel(const __grid_constant__ FrameTable t) {
+  const FrameStats& Fr = t.f[blockIdx.y];
+  const int B = Fr.bands;
+  const int i = blockIdx.x;
+  if (i >= B) return;
   __shared__ double s1[kRows];
   __shared__ double r[kRows];
   __shared__ int ex[kRows];
-  const int B = bands;
-  const int i = blockIdx.x;
+  const double* fsum = Fr.fsum;
+  const StatsState* st = Fr.state;
+  double* moments = Fr.moments;
   auto F = [&](int row, int col) { return fsum[static_cast<size_t>(col) * kRows + row]; };
   const double N = ldexp(F(B, B), -2 * kOnesExp);
   for (int j = threadIdx.x; j < B; j += blockDim.x) {
@@ -605,7 +805,10 @@ __global__ void __launch_bounds__(128) stats_finalize_kernel(const double* __res
   // row i, columns j <= i, mirrored, so the matrix is exactly symmetric
   for (int j = threadIdx.x; j <= i; j += blockDim.x) {
     double q = 0.5 * (F(i, j) + F(j, i));
-    if (i == j) q += static_cast<double>(st->l2sq[i]);  // the weight-1 diagonal, exact
+    if (i == j)
+      q += static_cast<double>(st->l2sq[i]);  // the weight-1 diagonal, exact
+    else  // the mean part of the weight-1 off-diagonal sums
+      q += static_cast<double>(st->l2sum[i]) * static_cast<double>(st->l2sum[j]) / N;
     const double s2 = ldexp(q, -(ex[i] + ex[j]));
     const double v = s2 + r[i] * s1[j] + s1[i] * r[j] + N * r[i] * r[j];
     outer[static_cast<size_t>(i) * B + j] = v;
@@ -766,32 +969,18 @@ constexpr int kSimtSlices = 96;
 
 size_t align256(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
 
-struct StatsWorkspace {
-  StatsState* state;
-  double* partials;
-  double* fsum;
-};
-
-size_t tensor_ws_bytes() {
-  return align256(sizeof(StatsState)) + align256(static_cast<size_t>(kMaxCtas) * kRows * kRows * sizeof(double)) +
-         align256(kRows * kRows * sizeof(double));
+// Tensor path, a group of m frames: m states, m F matrices, and the pieces'
+// partial slots (at most one per CTA plus one per frame boundary).
+size_t tensor_ws_bytes(int m) {
+  return static_cast<size_t>(m) * align256(sizeof(StatsState)) +
+         static_cast<size_t>(m) * align256(kRows * kRows * sizeof(double)) +
+         static_cast<size_t>(kMaxCtas + m) * kSlotElems * sizeof(long long);
 }
 
 size_t simt_ws_bytes(int bands) {
   const int n = ((bands + 1 + kSimtTile - 1) / kSimtTile) * kSimtTile;
   return align256(sizeof(StatsState)) + align256(static_cast<size_t>(kSimtSlices) * n * n * sizeof(double)) +
          align256(static_cast<size_t>(n) * n * sizeof(double));
-}
-
-StatsWorkspace carve(void* base, size_t partial_bytes) {
-  unsigned char* p = static_cast<unsigned char*>(base);
-  StatsWorkspace w;
-  w.state = reinterpret_cast<StatsState*>(p);
-  p += align256(sizeof(StatsState));
-  w.partials = reinterpret_cast<double*>(p);
-  p += align256(partial_bytes);
-  w.fsum = reinterpret_cast<double*>(p);
-  return w;
 }
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -810,27 +999,77 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-template <typename T>
-void launch_shift(const void* cube, int64_t P, int64_t stride, int B, const float* reference, StatsState* st,
-                  cudaStream_t s) {
-  shift_init_kernel<<<1, 256, 0, s>>>(st);
-  shift_partial_kernel<T><<<dim3(B, kShiftSplit), 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, st);
-  shift_finalize_kernel<<<1, 256, 0, s>>>(B, reference, st);
+FrameStats frame_of_job(const hsi_moments_job& j) {
+  FrameStats F{};
+  F.cube = j.cube;
+  F.pixels = static_cast<int64_t>(j.height) * j.width;
+  F.stride = j.plane_stride;
+  F.reference = j.reference;
+  F.moments = j.moments;
+  F.bands = j.bands;
+  return F;
 }
 
-// shift + scale -> GEMM -> (conditional) rescale + GEMM re-run -> reduce -> finalize
 template <typename T>
-int launch_tensor_stats(const void* cube, int64_t P, int B, int64_t stride, double* moments, const float* reference,
-                        void* workspace, cudaStream_t s, int* status) {
-  CUtensorMap map;
-  const int rc = encode_cube_map(&map, cube, sizeof(T) == 4 ? HSI_F32 : HSI_F16, P, B, stride, kBoxPx, kRows);
-  if (rc != HSI_OK) return rc;
-  const StatsWorkspace w = carve(workspace, static_cast<size_t>(kMaxCtas) * kRows * kRows * sizeof(double));
-  launch_shift<T>(cube, P, stride, B, reference, w.state, s);
-  const int64_t nkb = div_up<int64_t>(P, kKB);
+void launch_shift(const FrameTable& t, cudaStream_t s) {
+  shift_init_kernel<<<t.n, 256, 0, s>>>(t);
+  shift_partial_kernel<T><<<dim3(t.max_bands, kShiftSplit, t.n), 256, 0, s>>>(t);
+  shift_finalize_kernel<<<t.n, 256, 0, s>>>(t);
+}
+
+// One launch sequence for m <= kMaxBatch frames of element type T, all on the
+// tensor path: shift + scale -> GEMM -> (conditional) range + rescale + GEMM
+// re-run -> exact reduction -> finalize.
+template <typename T>
+int launch_tensor_group(const hsi_moments_job* const* jobs, int m, void* workspace, cudaStream_t s,
+                        int* status) {
+  static GemmParams p;  // large (13 KB): kept off the stack; calls are serialised by the caller's thread
+  p = GemmParams{};
+  FrameTable& t = p.t;
+  t.n = m;
+  t.status = status;
+  int64_t total = 0;
+  for (int f = 0; f < m; ++f) {
+    t.f[f] = frame_of_job(*jobs[f]);
+    t.f[f].kb_begin = total;
+    total += div_up<int64_t>(t.f[f].pixels, kKB);
+    if (t.f[f].bands > t.max_bands) t.max_bands = t.f[f].bands;
+    const int rc = encode_cube_map(&p.maps[f], jobs[f]->cube, jobs[f]->dtype, t.f[f].pixels, t.f[f].bands,
+                                   t.f[f].stride, kBoxPx, kRows);
+    if (rc != HSI_OK) return rc;
+  }
+  t.total_kb = total;
   int grid = num_sms();
   if (grid > kMaxCtas) grid = kMaxCtas;
-  if (nkb < grid) grid = static_cast<int>(nkb);
+  if (total < grid) grid = static_cast<int>(total);
+  t.ctas = grid;
+  // carve: states, F matrices, slots
+  unsigned char* w = static_cast<unsigned char*>(workspace);
+  long long* slots =
+      reinterpret_cast<long long*>(w + static_cast<size_t>(m) * (align256(sizeof(StatsState)) +
+                                                                 align256(kRows * kRows * sizeof(double))));
+  int used = 0;
+  for (int f = 0; f < m; ++f) {
+    FrameStats& F = t.f[f];
+    F.state = reinterpret_cast<StatsState*>(w + static_cast<size_t>(f) * align256(sizeof(StatsState)));
+    F.fsum = reinterpret_cast<double*>(w + static_cast<size_t>(m) * align256(sizeof(StatsState)) +
+                                       static_cast<size_t>(f) * align256(kRows * kRows * sizeof(double)));
+    // CTAs c whose range [total*c/grid, total*(c+1)/grid) meets [kb_begin, kb_end)
+    const int64_t k0 = F.kb_begin, k1 = F.kb_begin + div_up<int64_t>(F.pixels, kKB);
+    int lo = -1, hi = -1;
+    for (int c = 0; c < grid; ++c) {
+      const int64_t c0 = total * c / grid, c1 = total * (c + 1) / grid;
+      if (c1 > k0 && c0 < k1) {
+        if (lo < 0) lo = c;
+        hi = c;
+      }
+    }
+    F.cta_lo = lo;
+    F.nslots = hi - lo + 1;
+    F.slots = slots + static_cast<size_t>(used) * kSlotElems;
+    used += F.nslots;
+  }
+  if (used > kMaxCtas + m) return HSI_E_CAPACITY;  // cannot happen: pieces <= CTAs + frames - 1
   const StatsSmem L = stats_smem<T>();
   static bool configured = false;
   if (!configured) {
@@ -839,44 +1078,119 @@ int launch_tensor_stats(const void* cube, int64_t P, int B, int64_t stride, doub
     if (e != cudaSuccess) return static_cast<int>(e);
     configured = true;
   }
-  StatsArgs a;
-  a.pixels = P;
-  a.bands = B;
-  a.state = w.state;
-  a.partials = w.partials;
-  a.conditional = 0;
-  a.status = status;
-  stats_gemm_kernel<T><<<grid, kThreads, L.total, s>>>(map, a);
-  rescale_kernel<<<1, 128, 0, s>>>(B, w.state);
-  a.conditional = 1;
-  stats_gemm_kernel<T><<<grid, kThreads, L.total, s>>>(map, a);
-  stats_reduce_kernel<<<kRows * kRows / 32, 256, 0, s>>>(w.partials, grid, w.fsum);
-  stats_finalize_kernel<<<B, 128, 0, s>>>(w.fsum, w.state, B, moments);
+  launch_shift<T>(t, s);
+  p.conditional = 0;
+  stats_gemm_kernel<T><<<grid, kThreads, L.total, s>>>(p);
+  range_kernel<T><<<4 * num_sms(), 256, 0, s>>>(t);
+  rescale_kernel<<<m, 128, 0, s>>>(t);
+  p.conditional = 1;
+  stats_gemm_kernel<T><<<grid, kThreads, L.total, s>>>(p);
+  stats_reduce_kernel<<<dim3(kRows * kRows / 256, m), 256, 0, s>>>(t);
+  stats_finalize_kernel<<<dim3(t.max_bands, m), 128, 0, s>>>(t);
   return static_cast<int>(cudaGetLastError());
 }
 
 template <typename T>
-int launch_simt_stats(const void* cube, int64_t P, int B, int64_t stride, double* moments, const float* reference,
-                      void* workspace, cudaStream_t s) {
+int launch_simt_stats(const hsi_moments_job& j, void* workspace, cudaStream_t s) {
+  const int B = j.bands;
+  const int64_t P = static_cast<int64_t>(j.height) * j.width;
   const int tiles = (B + 1 + kSimtTile - 1) / kSimtTile;
   const int n = tiles * kSimtTile;
-  const StatsWorkspace w = carve(workspace, static_cast<size_t>(kSimtSlices) * n * n * sizeof(double));
-  launch_shift<T>(cube, P, stride, B, reference, w.state, s);
+  unsigned char* w = static_cast<unsigned char*>(workspace);
+  StatsState* state = reinterpret_cast<StatsState*>(w);
+  double* partials = reinterpret_cast<double*>(w + align256(sizeof(StatsState)));
+  double* fsum = reinterpret_cast<double*>(w + align256(sizeof(StatsState)) +
+                                           align256(static_cast<size_t>(kSimtSlices) * n * n * sizeof(double)));
+  static FrameTable t;  // 5.7 KB: kept off the stack
+  t = FrameTable{};
+  t.n = 1;
+  t.max_bands = B;
+  t.center_mean = 1;
+  t.f[0] = frame_of_job(j);
+  t.f[0].state = state;
+  launch_shift<T>(t, s);
   const dim3 grid(kSimtSlices, tiles * (tiles + 1) / 2);
-  stats_simt_kernel<T><<<grid, 256, 0, s>>>(static_cast<const T*>(cube), P, stride, B, w.state, w.partials,
+  stats_simt_kernel<T><<<grid, 256, 0, s>>>(static_cast<const T*>(j.cube), P, j.plane_stride, B, state, partials,
                                            kSimtSlices);
-  simt_reduce_kernel<<<(n * n + 255) / 256, 256, 0, s>>>(w.partials, kSimtSlices, n, w.fsum);
-  simt_finalize_kernel<<<1, 256, 0, s>>>(w.fsum, n, w.state, B, moments);
+  simt_reduce_kernel<<<(n * n + 255) / 256, 256, 0, s>>>(partials, kSimtSlices, n, fsum);
+  simt_finalize_kernel<<<1, 256, 0, s>>>(fsum, n, state, B, j.moments);
   return static_cast<int>(cudaGetLastError());
 }
 
-int check_common(const void* cube, int height, int width, int bands, int dtype, int64_t stride, double* moments) {
-  if (!cube || !moments || height <= 0 || width <= 0 || bands <= 0 || bands > HSI_MAX_BANDS) return HSI_E_INVALID;
-  if (dtype != HSI_F32 && dtype != HSI_F16) return HSI_E_INVALID;
-  const int64_t P = static_cast<int64_t>(height) * width;
-  if (stride < P || (stride & 7) != 0) return HSI_E_INVALID;
-  if ((reinterpret_cast<uintptr_t>(cube) & 15u) != 0) return HSI_E_INVALID;
+int check_job(const hsi_moments_job& j) {
+  if (!j.cube || !j.moments || j.height <= 0 || j.width <= 0 || j.bands <= 0 || j.bands > HSI_MAX_BANDS)
+    return HSI_E_INVALID;
+  if (j.dtype != HSI_F32 && j.dtype != HSI_F16) return HSI_E_INVALID;
+  const int64_t P = static_cast<int64_t>(j.height) * j.width;
+  if (j.plane_stride < P || (j.plane_stride & 7) != 0) return HSI_E_INVALID;
+  if ((reinterpret_cast<uintptr_t>(j.cube) & 15u) != 0) return HSI_E_INVALID;
   return HSI_OK;
+}
+
+bool tensor_capable(const hsi_moments_job& j) {
+  const int64_t P = static_cast<int64_t>(j.height) * j.width;
+  return j.bands <= kMaxTensorBands && P < kTensorMaxPixels;
+}
+
+// Default routing: small frames (where the integer path's one approximation,
+// the off-diagonal sums of the lowest limbs' products, is largest relative to
+// the sums, and the work is cheap) and bands >= 128 take the FP32 CUDA-core path.
+bool tensor_default(const hsi_moments_job& j) {
+  return tensor_capable(j) && static_cast<int64_t>(j.height) * j.width >= kTensorMinPixels;
+}
+
+enum class Route { kDefault, kSimt, kTensor };
+
+std::mutex g_stats_mutex;  // the launch helpers keep their large parameter blocks in statics
+
+int run_jobs(const hsi_moments_job* jobs, int n, void* ws, size_t ws_bytes, cudaStream_t s, Route route) {
+  if (!jobs || n <= 0) return HSI_E_INVALID;
+  for (int i = 0; i < n; ++i) {
+    const int rc = check_job(jobs[i]);
+    if (rc != HSI_OK) return rc;
+    if (route == Route::kTensor && !tensor_capable(jobs[i])) return HSI_E_CAPACITY;
+  }
+  if (!ws || ws_bytes < hsi_scene_moments_batch_workspace_bytes(jobs, n)) return HSI_E_WORKSPACE;
+  std::lock_guard<std::mutex> lock(g_stats_mutex);
+  const hsi_moments_job* group[2][kMaxBatch];
+  int count[2] = {0, 0};
+  auto flush = [&](int d) -> int {
+    if (count[d] == 0) return HSI_OK;
+    const int rc = d == 0 ? launch_tensor_group<float>(group[0], count[0], ws, s, nullptr)
+                          : launch_tensor_group<__half>(group[1], count[1], ws, s, nullptr);
+    count[d] = 0;
+    return rc;
+  };
+  for (int i = 0; i < n; ++i) {
+    const hsi_moments_job& j = jobs[i];
+    const bool tensor = route == Route::kTensor || (route == Route::kDefault && tensor_default(j));
+    int rc = HSI_OK;
+    if (tensor) {
+      const int d = j.dtype == HSI_F32 ? 0 : 1;
+      group[d][count[d]++] = &j;
+      if (count[d] == kMaxBatch) rc = flush(d);
+    } else {
+      rc = j.dtype == HSI_F32 ? launch_simt_stats<float>(j, ws, s) : launch_simt_stats<__half>(j, ws, s);
+    }
+    if (rc != HSI_OK) return rc;
+  }
+  int rc = flush(0);
+  if (rc == HSI_OK) rc = flush(1);
+  return rc;
+}
+
+hsi_moments_job single_job(const void* cube, int height, int width, int bands, int dtype, int64_t stride,
+                           double* moments, const float* reference) {
+  hsi_moments_job j{};
+  j.cube = cube;
+  j.plane_stride = stride;
+  j.moments = moments;
+  j.reference = reference;
+  j.height = height;
+  j.width = width;
+  j.bands = bands;
+  j.dtype = dtype;
+  return j;
 }
 
 }  // namespace
@@ -921,58 +1235,53 @@ int encode_cube_map_sw128(CUtensorMap* map, const void* cube, int dtype, int64_t
 
 using namespace hsi_b200;
 
+extern "C" HSI_API size_t hsi_scene_moments_batch_workspace_bytes(const hsi_moments_job* jobs, int num_jobs) {
+  if (!jobs || num_jobs <= 0) return 0;
+  size_t need = 0;
+  int tensor = 0;
+  for (int i = 0; i < num_jobs; ++i) {
+    if (jobs[i].bands <= 0 || jobs[i].bands > HSI_MAX_BANDS) return 0;
+    // every job may be routed either way (the _tc and _simt entry points force one)
+    const size_t b = simt_ws_bytes(jobs[i].bands);
+    if (b > need) need = b;
+    if (tensor_capable(jobs[i])) ++tensor;
+  }
+  if (tensor > 0) {
+    const size_t b = tensor_ws_bytes(tensor < kMaxBatch ? tensor : kMaxBatch);
+    if (b > need) need = b;
+  }
+  return need;
+}
+
+extern "C" HSI_API int hsi_scene_moments_batch(const hsi_moments_job* jobs, int num_jobs, void* d_workspace,
+                                               size_t workspace_bytes, hsi_stream_t stream) {
+  return run_jobs(jobs, num_jobs, d_workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream),
+                  Route::kDefault);
+}
+
 extern "C" HSI_API size_t hsi_stats_workspace_bytes(int height, int width, int bands) {
   if (height <= 0 || width <= 0 || bands <= 0 || bands > HSI_MAX_BANDS) return 0;
-  const size_t a = tensor_ws_bytes(), b = simt_ws_bytes(bands);
+  const size_t a = tensor_ws_bytes(1), b = simt_ws_bytes(bands);
   return a > b ? a : b;
 }
 
 extern "C" HSI_API int hsi_scene_moments(const void* d_cube, int height, int width, int bands, int dtype,
                                          int64_t plane_stride, double* d_moments, const float* d_reference,
                                          void* d_workspace, size_t workspace_bytes, hsi_stream_t stream) {
-  const int rc = check_common(d_cube, height, width, bands, dtype, plane_stride, d_moments);
-  if (rc != HSI_OK) return rc;
-  if (!d_workspace || workspace_bytes < hsi_stats_workspace_bytes(height, width, bands)) return HSI_E_WORKSPACE;
-  const int64_t P = static_cast<int64_t>(height) * width;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  // The integer path's one approximation (the off-diagonal sums of the
-  // lowest limbs' products) shrinks as 1/sqrt(pixels); small frames, which
-  // are also cheap, take the FP32 CUDA-core path.
-  if (bands <= kMaxTensorBands && P >= kTensorMinPixels) {
-    return dtype == HSI_F32 ? launch_tensor_stats<float>(d_cube, P, bands, plane_stride, d_moments, d_reference,
-                                                         d_workspace, s, nullptr)
-                            : launch_tensor_stats<__half>(d_cube, P, bands, plane_stride, d_moments, d_reference,
-                                                          d_workspace, s, nullptr);
-  }
-  return dtype == HSI_F32
-             ? launch_simt_stats<float>(d_cube, P, bands, plane_stride, d_moments, d_reference, d_workspace, s)
-             : launch_simt_stats<__half>(d_cube, P, bands, plane_stride, d_moments, d_reference, d_workspace, s);
+  const hsi_moments_job j = single_job(d_cube, height, width, bands, dtype, plane_stride, d_moments, d_reference);
+  return run_jobs(&j, 1, d_workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream), Route::kDefault);
 }
 
 extern "C" HSI_API int hsi_scene_moments_simt(const void* d_cube, int height, int width, int bands, int dtype,
                                               int64_t plane_stride, double* d_moments, const float* d_reference,
                                               void* d_workspace, size_t workspace_bytes, hsi_stream_t stream) {
-  const int rc = check_common(d_cube, height, width, bands, dtype, plane_stride, d_moments);
-  if (rc != HSI_OK) return rc;
-  if (!d_workspace || workspace_bytes < hsi_stats_workspace_bytes(height, width, bands)) return HSI_E_WORKSPACE;
-  const int64_t P = static_cast<int64_t>(height) * width;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  return dtype == HSI_F32
-             ? launch_simt_stats<float>(d_cube, P, bands, plane_stride, d_moments, d_reference, d_workspace, s)
-             : launch_simt_stats<__half>(d_cube, P, bands, plane_stride, d_moments, d_reference, d_workspace, s);
+  const hsi_moments_job j = single_job(d_cube, height, width, bands, dtype, plane_stride, d_moments, d_reference);
+  return run_jobs(&j, 1, d_workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream), Route::kSimt);
 }
 
 extern "C" HSI_API int hsi_scene_moments_tc(const void* d_cube, int height, int width, int bands, int dtype,
                                             int64_t plane_stride, double* d_moments, const float* d_reference,
                                             void* d_workspace, size_t workspace_bytes, hsi_stream_t stream) {
-  const int rc = check_common(d_cube, height, width, bands, dtype, plane_stride, d_moments);
-  if (rc != HSI_OK) return rc;
-  if (bands > kMaxTensorBands) return HSI_E_CAPACITY;
-  if (!d_workspace || workspace_bytes < hsi_stats_workspace_bytes(height, width, bands)) return HSI_E_WORKSPACE;
-  const int64_t P = static_cast<int64_t>(height) * width;
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  return dtype == HSI_F32 ? launch_tensor_stats<float>(d_cube, P, bands, plane_stride, d_moments, d_reference,
-                                                       d_workspace, s, nullptr)
-                          : launch_tensor_stats<__half>(d_cube, P, bands, plane_stride, d_moments, d_reference,
-                                                        d_workspace, s, nullptr);
+  const hsi_moments_job j = single_job(d_cube, height, width, bands, dtype, plane_stride, d_moments, d_reference);
+  return run_jobs(&j, 1, d_workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream), Route::kTensor);
 }

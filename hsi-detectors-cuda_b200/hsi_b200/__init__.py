@@ -129,6 +129,8 @@ def _optional_symbols(L):
         "hsi_scene_moments": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
         "hsi_scene_moments_simt": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
         "hsi_scene_moments_tc": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
+        "hsi_scene_moments_batch_workspace_bytes": ([C.POINTER(MomentsJob), i32], C.c_size_t),
+        "hsi_scene_moments_batch": ([C.POINTER(MomentsJob), i32, vp, C.c_size_t, vp], i32),
         "hsi_statistics_elements": ([i32, i32], C.c_size_t),
         "hsi_factor_workspace_bytes": ([i32, i32], C.c_size_t),
         "hsi_build_statistics": ([i32, i32, i32, f64, vp, vp, i64, vp, vp, vp, vp, vp, C.c_size_t, vp], i32),
@@ -371,6 +373,31 @@ def scene_moments(cube, height, width, bands, dtype=F32, stride=None, out=None, 
     check(fn(_ptr(cube), height, width, bands, dtype, stride, _ptr(out), _ptr(reference), _ptr(workspace),
              workspace.numel(), _stream(stream)), "hsi_scene_moments")
     return out
+
+
+class MomentsJob(C.Structure):
+    """hsi_moments_job: one frame of hsi_scene_moments_batch."""
+    _fields_ = [("cube", C.c_void_p), ("plane_stride", C.c_int64), ("moments", C.c_void_p),
+                ("reference", C.c_void_p), ("height", C.c_int32), ("width", C.c_int32), ("bands", C.c_int32),
+                ("dtype", C.c_int32)]
+
+
+def moments_job(cube, height, width, bands, out, dtype=F32, stride=None, reference=None) -> MomentsJob:
+    stride = cube.shape[-1] if stride is None else stride
+    return MomentsJob(_ptr(cube), stride, _ptr(out), _ptr(reference), height, width, bands, dtype)
+
+
+def scene_moments_batch(jobs, workspace=None, stream=None, device="cuda"):
+    """Raw moments of many frames (MomentsJob list) with hsi_scene_moments_batch:
+    the tensor-path frames run as one launch sequence per element type."""
+    torch = _torch()
+    arr = (MomentsJob * len(jobs))(*jobs)
+    need = lib().hsi_scene_moments_batch_workspace_bytes(arr, len(jobs))
+    if workspace is None:
+        workspace = torch.empty(max(need, 1), dtype=torch.uint8, device=device)
+    check(lib().hsi_scene_moments_batch(arr, len(jobs), _ptr(workspace), workspace.numel(), _stream(stream)),
+          "hsi_scene_moments_batch")
+    return workspace
 
 
 def split_moments(m, bands):

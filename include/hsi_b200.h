@@ -208,6 +208,26 @@ HSI_API int hsi_scene_moments_tc(const void* d_cube, int height, int width, int 
                                  int64_t plane_stride, double* d_moments, const float* d_reference,
                                  void* d_workspace, size_t workspace_bytes, hsi_stream_t stream);
 
+/* Moments of many frames at once: each job's output is what
+ * hsi_scene_moments gives for that frame alone (the tensor path's sums are
+ * exact integers until the final FP64 rebuild, so they do not depend on how
+ * frames are grouped).  Frames on the tensor path are grouped by element type,
+ * up to 64 per group, and each group runs as one launch sequence: a persistent
+ * GEMM over all of the group's pixels plus one launch per small step for all
+ * frames.  Other frames run one by one on the FP32 path.  Frames of any sizes
+ * and band counts may be mixed.  The workspace serves one group at a time
+ * (stream order), so its size does not grow past 64 tensor frames. */
+typedef struct hsi_moments_job {
+  const void* cube;        /* device BSQ cube, 16-byte aligned */
+  int64_t plane_stride;    /* elements between band planes (>= height*width, multiple of 8) */
+  double* moments;         /* out: B + B*B + 1 doubles */
+  const float* reference;  /* nullable: `bands` floats, the shift r */
+  int32_t height, width, bands, dtype;
+} hsi_moments_job;
+HSI_API size_t hsi_scene_moments_batch_workspace_bytes(const hsi_moments_job* jobs, int num_jobs);
+HSI_API int hsi_scene_moments_batch(const hsi_moments_job* jobs, int num_jobs, void* d_workspace,
+                                    size_t workspace_bytes, hsi_stream_t stream);
+
 /* ---- detector statistics (FP64 factorisation) --------------------------------
  * For each of `num_frames` frames (moments contiguous, B + B*B + 1 doubles
  * each) build the statistics of reference build_statistics

@@ -61,6 +61,28 @@ def test_random_plateaus_bit_exact(hsi, orc, shape, radius, higher):
     assert _tuples(got) == _tuples(want)
 
 
+@pytest.mark.parametrize("radius", [1, 3, 4])
+@pytest.mark.parametrize("higher", [False, True])
+def test_sparse_and_dense_segments_bit_exact(hsi, orc, radius, higher):
+    """Rows alternate between few candidates (their windows read from global
+    memory) and many (the staged window with the separable window-best), so
+    both suppression paths meet at shared window rows."""
+    H, W = 96, 4500
+    rng = np.random.default_rng(1000 + radius)
+    q = rng.integers(0, 50, (H, W)) / 50.0
+    sparse_rows = (np.arange(H) // 3) % 2 == 0
+    # sparse rows: candidates only where a rare draw lifts the score past the threshold
+    rare = rng.random((H, W)) < 0.002
+    q[sparse_rows] = np.where(rare[sparse_rows], 0.98, q[sparse_rows] * 0.5)
+    score = (q if higher else 1.0 - q).astype(np.float32)
+    target = rng.integers(0, 8, H * W).astype(np.int32)
+    thr = 0.9 if higher else 0.1
+    n0, want = orc.detect(score.reshape(-1), target, H, W, thr, radius, higher, capacity=1 << 22)
+    n, got = _gpu_detect(hsi, score.reshape(-1), target, H, W, thr, radius, higher)
+    assert n == n0
+    assert _tuples(got) == _tuples(want)
+
+
 def test_capacity_overflow_keeps_raster_prefix(hsi, orc):
     H, W = 300, 301
     rng = np.random.default_rng(5)
