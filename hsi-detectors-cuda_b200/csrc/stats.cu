@@ -66,7 +66,10 @@ namespace hsi_b200 {
 namespace {
 
 constexpr int kKB = 128;         // pixels per K-block (one INT8 operand row)
-constexpr int kBoxPx = 64;       // pixels per TMA box
+constexpr int kBoxPx = 128;      // pixels per TMA box: 512-byte runs of each band plane
+constexpr int kHalfPx = 64;      // pixels a converter pass covers (half a K-block)
+constexpr int kBoxesPerKB = kKB / kBoxPx;
+constexpr int kHalvesPerBox = kBoxPx / kHalfPx;
 constexpr int kChunkKB = 256;    // K-blocks per INT32 chunk: 32768 px, no overflow
 constexpr int kRows = 128;       // band rows of the GEMM (bands + ones row)
 constexpr int kOpStages = 2;
@@ -101,10 +104,10 @@ constexpr uint32_t kExpBits = 0x4B000000u;     // bits of 2^23
 constexpr uint32_t kZeroBits = 0x4B408080u;    // y for q = 0
 constexpr uint32_t kOnesBits = 0x4B418080u;    // y for q = 2^16 (the ones row)
 
-// Input stages hold one TMA box (half a K-block: 64 pixels x 128 bands).
+// Input stages hold one TMA box (kBoxPx pixels x 128 bands), 128 KB in all.
 template <typename T>
 constexpr int in_stages() {
-  return sizeof(T) == 4 ? 4 : 8;
+  return 131072 / (kRows * kBoxPx * static_cast<int>(sizeof(T)));
 }
 template <typename T>
 constexpr int in_tile_bytes() {
@@ -288,7 +291,7 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
         prefetch_tensormap(map);
         const int64_t kbf = t.f[f].kb_begin;
         for (int64_t kb = walk.lo(f); kb < walk.hi(f) && ok; ++kb) {
-          for (int half = 0; half < 2; ++half, ++box) {
+          for (int half = 0; half < kBoxesPerKB; ++half, ++box) {
             const int s = box % kInStages;
             const uint32_t ph = (box / kInStages) & 1u;
             if (*abort_flag || !mbar_wait(&in_empty[s], ph ^ 1u)) {
@@ -378,7 +381,7 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
     // maps to o ^ 64
     const int band0 = (cw >> 2) * 8 + (cw & 3) + 4 * sub;
     const uint32_t o0 = sw128_byte(band0, lp);
-    uint32_t box = 0, i = 0;
+    uint32_t i = 0;
     bool aborted = false;
     for (int f = walk.first(); !aborted && walk.in_range(f); ++f) {
       if (walk.skip(f)) continue;
@@ -429,9 +432,11 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
         const int so = i % kOpStages;
         unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kLimbBytes;
 #pragma unroll
-        for (int half = 0; half < 2; ++half, ++box) {
+        for (int half = 0; half < 2; ++half) {
+          const uint32_t box = i * kBoxesPerKB + half / kHalvesPerBox;  // input box of this half
           const int s = box % kInStages;
-          if (!mbar_wait(&in_full[s], (box / kInStages) & 1u) ||
+          const int sub_off = (half % kHalvesPerBox) * kHalfPx;         // its pixels within the box
+          if ((sub_off == 0 && !mbar_wait(&in_full[s], (box / kInStages) & 1u)) ||
               (half == 0 && !mbar_wait(&op_empty[so], ((i / kOpStages) & 1u) ^ 1u))) {
             record_error(t.status, HSI_E_TIMEOUT);
             *abort_flag = 1;
@@ -439,14 +444,14 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
             break;
           }
           const T* in = reinterpret_cast<const T*>(smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>());
-          const int64_t gp = (kb - F.kb_begin) * kKB + half * kBoxPx + lp;
+          const int64_t gp = (kb - F.kb_begin) * kKB + half * kHalfPx + lp;
           const int nvalid = gp >= P ? 0 : (P - gp >= 4 ? 4 : static_cast<int>(P - gp));
 #pragma unroll
           for (int t2 = 0; t2 < kSlots; ++t2) {
             const int b = band0 + 32 * t2;
             uint32_t y[4] = {kZeroBits, kZeroBits, kZeroBits, kZeroBits};
             if (b < B) {
-              const float4 x = load4f<T>(in + b * kBoxPx + lp);
+              const float4 x = load4f<T>(in + b * kBoxPx + sub_off + lp);
               const float xv[4] = {x.x, x.y, x.z, x.w};
               // fully unrolled with a predicate: a loop bounded by nvalid would
               // index y[] dynamically and move it to local memory
@@ -477,7 +482,7 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
             *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + o) = l2;
           }
           __syncwarp();
-          if (lane == 0) mbar_arrive(&in_empty[s]);
+          if (lane == 0 && sub_off + kHalfPx == kBoxPx) mbar_arrive(&in_empty[s]);
           if (half == 1) {
             fence_proxy_async_smem();
             __syncwarp();
@@ -559,7 +564,7 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
 
 // ---------------------------------------------------------------------------
 // Reference point and fixed-point scale per band from a regular subsample
-// (every 16th run of 64 pixels on large frames): r = the midpoint of the
+// (about 256 evenly spaced runs of 64 pixels on frames above 512 runs): r = the midpoint of the
 // subsample's range (which minimises its largest |x - r|, and, being built
 // from a minimum and a maximum, does not depend on the order the blocks
 // finish in), e such that that largest |x - r| maps to 2^20 (4x headroom
@@ -629,7 +634,7 @@ __device__ void fold_subsample(double sum, double cnt, float lo, float hi, Stats
 }
 
 // Subsample statistics, grid (bands, kShiftSplit, frames): runs of 64
-// pixels, every 16th run on large frames.
+// pixels, about 256 of them per band on frames above 512 runs.
 template <typename T>
 __global__ void __launch_bounds__(256) shift_partial_kernel(const __grid_constant__ FrameTable t) {
   const FrameStats& F = t.f[blockIdx.z];
@@ -638,7 +643,7 @@ __global__ void __launch_bounds__(256) shift_partial_kernel(const __grid_constan
   const T* plane = static_cast<const T*>(F.cube) + static_cast<int64_t>(b) * F.stride;
   const int64_t pixels = F.pixels;
   const int64_t runs = div_up<int64_t>(pixels, 64);
-  const int64_t step = runs > 4096 ? 16 : 1;
+  const int64_t step = runs > 512 ? runs / 256 : 1;  // about 256 runs (16384 pixels) per band
   const int64_t sampled = div_up<int64_t>(runs, step);
   const int64_t r0 = sampled * blockIdx.y / kShiftSplit, r1 = sampled * (blockIdx.y + 1) / kShiftSplit;
   double sum = 0.0, cnt = 0.0;

@@ -88,8 +88,8 @@ def test_out_of_range_frame_is_rerun_alone(hsi, orc):
     specs = [(113, 512, 600, 0), (113, 512, 600, 0), (113, 512, 600, 0)]
     cubes = [_frame(hsi, B, H, W, dt, 0x5EED7200 + i) for i, (B, H, W, dt) in enumerate(specs)]
     P = 512 * 600
-    # frames above 4096 runs of 64 pixels sample every 16th run: pixels
-    # 64..1023 are never in the subsample
+    # frames above 512 runs of 64 pixels sample every (runs // 256)-th run,
+    # here every 18th: pixels 64..1151 are never in the subsample
     cubes[1][5, 100] = 500.0
     cubes[1][70, 64] = -300.0
     got = _run_batch(hsi, specs, cubes)
