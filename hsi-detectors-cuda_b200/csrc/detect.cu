@@ -2,14 +2,21 @@
 //
 // Three launches for a whole batch of score maps, no atomics on the data
 // path, so every list comes out in raster order and is identical run to run:
-//   1. flags:  per row segment (up to 2048 pixels of one row), every pixel's
-//              pass/fail as warp ballot words (bitmask in the workspace) and
-//              the segment's count.  The score rows the NMS window needs are
-//              staged in shared memory (radius <= 4; larger radii read global
-//              memory), padded with NaN so out-of-frame neighbours never win
-//              or tie, exactly like the bounds checks of the CPU loop;
-//   2. scan:   one block per map turns segment counts into output offsets,
-//              starting at the caller's *count, and advances *count;
+//   1. flags:  per tile of 256 columns x 64 rows of one map, every pixel's
+//              pass/fail as warp ballot words (a bitmask in the workspace:
+//              one word per 32 pixels of a 2048-pixel row segment).  The
+//              map's rows stream through a shared-memory ring (cp.async, four
+//              rows ahead).  Per row, each column's first-best score of the
+//              (2r+1)-row window (better score, then lower row) is found
+//              once; a candidate passes when none of the 2r+1 column bests
+//              around it comes first in the window's order (better score,
+//              then lower linear index).  Out-of-frame neighbours are NaN,
+//              which never win or tie, exactly like the bounds checks of the
+//              CPU loop.  Radii above 8 read each candidate's window from
+//              global memory instead;
+//   2. scan:   one block per map counts each row segment's passing pixels
+//              (popcounts of its mask words), turns the counts into output
+//              offsets starting at the caller's *count, and advances *count;
 //   3. emit:   each segment writes its detections at offset + in-segment
 //              rank, dropping (but having counted) those past capacity.
 // Semantics are the reference CPU path's (src/sam_cpu.cpp:86-138), polarity
@@ -22,16 +29,19 @@
 namespace hsi_b200 {
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 256;                // scan / emit blocks
 constexpr int kPerThread = 8;
-constexpr int kSeg = kThreads * kPerThread;  // 2048 pixels per segment
+constexpr int kSeg = kThreads * kPerThread;  // 2048 pixels per row segment
 constexpr int kWordsPerSeg = kSeg / 32;      // 64
-constexpr int kMaxStagedRadius = 4;
-constexpr int kColsPerThread = (kSeg + 2 * kMaxStagedRadius + kThreads - 1) / kThreads;  // 9
-// Segments with at most this many threads holding a candidate skip the staged
-// window and read their candidates' neighbourhoods from global memory.
-constexpr int kSparseThreads = 64;
 constexpr int kMaxJobs = 64;
+// flags tiles
+constexpr int kTileW = 256;                        // columns per tile (8 ballot warps)
+constexpr int kTileH = 64;                         // rows per tile
+constexpr int kMaxRingR = 8;                       // largest radius streamed through the ring
+constexpr int kAhead = 4;                          // rows in flight ahead of the window
+constexpr int kRing = 2 * kMaxRingR + 2 + kAhead;  // ring rows: window, one spare, rows in flight
+constexpr int kRingCols = kTileW + 2 * kMaxRingR;  // 272
+constexpr int kFlagThreads = 288;                  // >= kRingCols, whole warps
 
 struct Job {
   const float* score;
@@ -45,12 +55,15 @@ struct Job {
   uint32_t* count;
   int seg0;          // first segment of this map in the batch
   int segs_per_row;  // ceil(width / kSeg)
+  int tile0;         // first flags tile of this map in the batch
+  int tiles_x;       // ceil(width / kTileW)
 };
 
 struct Batch {
   Job jobs[kMaxJobs];
   int njobs;
   int total_segs;
+  int total_tiles;
   uint32_t* counts;   // [total_segs]
   uint32_t* offsets;  // [total_segs]
   uint32_t* masks;    // [total_segs * 64]
@@ -65,20 +78,36 @@ __device__ __forceinline__ int find_job(const Batch& b, int seg) {
   return lo;
 }
 
-__device__ __forceinline__ bool better(float a, float b, bool higher) { return higher ? a > b : a < b; }
-
-// The total order of the suppression window: the better score first (by
-// polarity), then the lower linear index; NaN (outside the frame) is last.
-// A candidate survives exactly when it is the first of its window.  Inside a
-// staged window the position ry * tw + c orders pixels as their linear
-// indices do (row first, c < tw), so it stands in for the index.
-__device__ __forceinline__ bool lex_first(float av, int ai, float bv, int bi, bool higher) {
-  if (isnan(bv)) return !isnan(av);
-  if (isnan(av)) return false;
-  return better(av, bv, higher) || (av == bv && ai < bi);
+__device__ __forceinline__ int find_job_tile(const Batch& b, int tile) {
+  int lo = 0, hi = b.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (b.jobs[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
+  }
+  return lo;
 }
 
-// NMS against global memory, for radii too large to stage.
+__device__ __forceinline__ bool better(float a, float b, bool higher) { return higher ? a > b : a < b; }
+
+__device__ __forceinline__ bool over_threshold(float s, float threshold, bool higher) {
+  return higher ? s >= threshold : s <= threshold;  // NaN fails both
+}
+
+// Mask word of the 32 pixels of row y starting at column xw (a multiple of 32).
+__device__ __forceinline__ uint32_t* mask_word(const Batch& b, const Job& J, int y, int xw) {
+  return b.masks + static_cast<int64_t>(J.seg0 + y * J.segs_per_row + xw / kSeg) * kWordsPerSeg + (xw % kSeg) / 32;
+}
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// NMS against global memory, for radii too large for the ring.
 __device__ bool local_best_global(const float* __restrict__ s, int x, int y, int w, int h, int r, float self,
                                   bool higher) {
   const int64_t self_idx = static_cast<int64_t>(y) * w + x;
@@ -98,134 +127,121 @@ __device__ bool local_best_global(const float* __restrict__ s, int x, int y, int
   return true;
 }
 
-__global__ void __launch_bounds__(kThreads) flags_kernel(const __grid_constant__ Batch b) {
-  // (2r+1) rows x (kSeg + 2r) columns of scores (at least 3 rows: after the
-  // vertical pass rows 0 and 1 hold each column's best value and index)
-  extern __shared__ float tile[];
-  __shared__ uint32_t s_count[kThreads / 32];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int seg = blockIdx.x; seg < b.total_segs; seg += gridDim.x) {
-    __syncthreads();  // the previous segment is done with the tile and s_count
-    const Job& J = b.jobs[find_job(b, seg)];
-    const int local = seg - J.seg0;
-    const int y = local / J.segs_per_row;
-    const int x0 = (local % J.segs_per_row) * kSeg;
-    const int len = min(kSeg, J.width - x0);
-    const int r = J.radius > 0 ? J.radius : 0;
-    const bool staged = r <= kMaxStagedRadius;
+__global__ void __launch_bounds__(kFlagThreads) flags_kernel(const __grid_constant__ Batch b) {
+  __shared__ float ring[kRing][kRingCols];  // score rows, NaN outside the frame
+  __shared__ float s_v[2][kRingCols];       // per column: first-best score of the window (two rows)
+  __shared__ int s_k[2][kRingCols];         //   its row within the window (0 .. 2r)
+  __shared__ float s_c[2][kRingCols];       //   the centre row's score
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const float nan = __int_as_float(0x7fc00000);
+  for (int tile = blockIdx.x; tile < b.total_tiles; tile += gridDim.x) {
+    __syncthreads();  // the previous tile is done with the shared buffers
+    const Job& J = b.jobs[find_job_tile(b, tile)];
+    const int local = tile - J.tile0;
+    const int x0 = (local % J.tiles_x) * kTileW;
+    const int y0 = (local / J.tiles_x) * kTileH;
+    const int y1 = min(J.height, y0 + kTileH);
+    const int W = J.width, H = J.height;
     const bool higher = J.higher != 0;
-    const int tw = kSeg + 2 * r;
-    float* col_v = tile;                               // tile row 0, after the vertical pass
-    int* col_i = reinterpret_cast<int*>(tile + tw);    // tile row 1
-    // threshold first: a segment with few candidates checks their windows in
-    // global memory (L1/L2), one with many stages the whole window once
-    float sv[kPerThread];
-    uint32_t over_bits = 0;
-#pragma unroll
-    for (int i = 0; i < kPerThread; ++i) {
-      const int xi = i * kThreads + threadIdx.x;
-      sv[i] = 0.0f;
-      if (xi < len) {
-        sv[i] = J.score[static_cast<int64_t>(y) * J.width + x0 + xi];
-        if (higher ? (sv[i] >= J.threshold) : (sv[i] <= J.threshold)) over_bits |= 1u << i;
-      }
-    }
-    const int busy = __syncthreads_count(over_bits != 0);  // threads holding a candidate
-    const bool use_tile = r > 0 && staged && busy > kSparseThreads;
-    if (use_tile) {
-      // row by row, no index division; NaN outside the frame: never better, never equal
-      const float nan = __int_as_float(0x7fc00000);
-      for (int ry = 0; ry <= 2 * r; ++ry) {
-        const int gy = y - r + ry;
-        const bool row_in = gy >= 0 && gy < J.height;
-        const float* src = J.score + static_cast<int64_t>(row_in ? gy : 0) * J.width;
-        float* dst = tile + ry * tw;
-        for (int rx = threadIdx.x; rx < len + 2 * r; rx += kThreads) {
-          const int gx = x0 - r + rx;
-          dst[rx] = row_in && gx >= 0 && gx < J.width ? src[gx] : nan;
+    const float thr = J.threshold;
+    const int r = J.radius > 0 ? J.radius : 0;
+    if (r > kMaxRingR) {
+      for (int y = y0; y < y1; ++y) {
+        if (t >= kTileW) continue;
+        const int x = x0 + t;
+        bool pass = false;
+        if (x < W) {
+          const float s = J.score[static_cast<int64_t>(y) * W + x];
+          pass = over_threshold(s, thr, higher) && local_best_global(J.score, x, y, W, H, r, s, higher);
         }
+        const uint32_t word = __ballot_sync(0xffffffffu, pass);
+        if (lane == 0 && x0 + 32 * warp < W) *mask_word(b, J, y, x0 + 32 * warp) = word;
       }
-      __syncthreads();
-      // vertical pass: the first (score, index) of each staged column, kept in
-      // registers until every thread has read the tile, then written over its
-      // first two rows
-      float cv[kColsPerThread];
-      int ci[kColsPerThread];
-#pragma unroll
-      for (int k = 0; k < kColsPerThread; ++k) {
-        const int c = threadIdx.x + k * kThreads;
-        cv[k] = __int_as_float(0x7fc00000);
-        ci[k] = 0;
-        if (c < len + 2 * r) {
-          cv[k] = tile[c];
-          ci[k] = c;
-          for (int ry = 1; ry <= 2 * r; ++ry) {
-            const int id = ry * tw + c;
-            const float v = tile[id];
-            if (lex_first(v, id, cv[k], ci[k], higher)) {
-              cv[k] = v;
-              ci[k] = id;
+      continue;
+    }
+    const int ncols = kTileW + 2 * r;
+    const int cx = x0 - r + t;  // this thread's column in the vertical pass
+    const bool col_in = t < ncols && cx >= 0 && cx < W;
+    const int last = y1 - 1 + r;  // last row the tile reads
+    // One ring row per call: a 4-byte cp.async per in-frame column, NaN
+    // stored directly elsewhere, and one commit group per thread per call.
+    int next_row = y0 - r, next_slot = 0;
+    auto issue_next = [&]() {
+      if (next_row <= last && t < ncols) {
+        float* dst = &ring[next_slot][t];
+        if (col_in && next_row >= 0 && next_row < H)
+          cp_async4(dst, J.score + static_cast<int64_t>(next_row) * W + cx);
+        else
+          *dst = nan;
+      }
+      cp_async_commit();
+      ++next_row;
+      next_slot = next_slot + 1 == kRing ? 0 : next_slot + 1;
+    };
+    for (int k = 0; k < 2 * r + kAhead; ++k) issue_next();
+    int top_slot = 0;  // ring slot of row y - r
+    for (int y = y0; y <= y1; ++y) {
+      // row y + r + kAhead reuses the slot of row y - r - 2 or older, whose
+      // last reader passed the barrier of the previous iteration
+      if (y < y1) issue_next();
+      cp_async_wait<kAhead>();  // this thread's copies up to row y + r have landed
+      __syncthreads();          // ... and everyone's
+      if (y > y0 && t < kTileW) {
+        // candidates of row y - 1 against the column bests around them
+        const int yh = y - 1, hb = yh & 1;
+        const int x = x0 + t;
+        bool pass = false;
+        if (x < W) {
+          const float s = s_c[hb][t + r];
+          if (over_threshold(s, thr, higher)) {
+            pass = true;
+            for (int dx = -r; dx <= r; ++dx) {
+              const float v = s_v[hb][t + r + dx];
+              const int k = s_k[hb][t + r + dx];
+              // first in the window's order: better score, or the same score
+              // at a lower linear index (an earlier row, or this row to the left)
+              if (!isnan(v) && (better(v, s, higher) || (v == s && (k < r || (k == r && dx < 0))))) {
+                pass = false;
+                break;
+              }
             }
           }
         }
+        const uint32_t word = __ballot_sync(0xffffffffu, pass);
+        if (lane == 0 && x0 + 32 * warp < W) *mask_word(b, J, yh, x0 + 32 * warp) = word;
       }
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < kColsPerThread; ++k) {
-        const int c = threadIdx.x + k * kThreads;
-        if (c < len + 2 * r) {
-          col_v[c] = cv[k];
-          col_i[c] = ci[k];
-        }
-      }
-      __syncthreads();
-    }
-    uint32_t mine = 0;
-#pragma unroll
-    for (int i = 0; i < kPerThread; ++i) {
-      const int xi = i * kThreads + threadIdx.x;  // pixel within the segment
-      bool pass = false;
-      if ((over_bits >> i) & 1u) {
-        const int x = x0 + xi;
-        const float s = sv[i];
-        if (r == 0) {
-          pass = true;
-        } else if (use_tile) {
-          // first of the window = first of the column bests around it
-          const int self = r * tw + xi + r;  // tile position of the candidate
-          float bv = s;
-          int bi = self;
-          for (int dx = -r; dx <= r; ++dx) {
-            const float v = col_v[xi + r + dx];
-            const int id = col_i[xi + r + dx];
-            if (lex_first(v, id, bv, bi, higher)) {
-              bv = v;
-              bi = id;
-            }
+      if (y < y1 && t < ncols) {
+        // column t's first-best over rows y - r .. y + r
+        float bv = nan;
+        int bk = 0;
+        int sl = top_slot;
+        for (int k = 0; k <= 2 * r; ++k) {
+          const float v = ring[sl][t];
+          if (!isnan(v) && (isnan(bv) || better(v, bv, higher))) {
+            bv = v;
+            bk = k;
           }
-          pass = bi == self;
-        } else {
-          pass = local_best_global(J.score, x, y, J.width, J.height, r, s, higher);
+          if (k == r) s_c[y & 1][t] = v;
+          sl = sl + 1 == kRing ? 0 : sl + 1;
         }
+        s_v[y & 1][t] = bv;
+        s_k[y & 1][t] = bk;
       }
-      const uint32_t word = __ballot_sync(0xffffffffu, pass);
-      if (lane == 0) {
-        b.masks[static_cast<int64_t>(seg) * kWordsPerSeg + i * (kThreads / 32) + warp] = word;
-        mine += __popc(word);
-      }
-    }
-    if (lane == 0) s_count[warp] = mine;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t total = 0;
-      for (int w = 0; w < kThreads / 32; ++w) total += s_count[w];
-      b.counts[seg] = total;
+      top_slot = top_slot + 1 == kRing ? 0 : top_slot + 1;
     }
   }
 }
 
-// One block per map: exclusive scan of its segment counts from *count;
-// *count += total.
+// Passing pixels of segment `seg` of job J: popcount of its mask words that
+// cover pixels of the map (words past the row's end are never written).
+__device__ __forceinline__ int seg_words(const Job& J, int local) {
+  const int xs = (local % J.segs_per_row) * kSeg;
+  const int len = min(kSeg, J.width - xs);
+  return (len + 31) / 32;
+}
+
+// One block per map: segment counts from the masks, their exclusive scan from
+// *count; *count += total.
 __global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ Batch b) {
   __shared__ uint32_t s_warp[32];
   __shared__ uint32_t s_carry;
@@ -235,8 +251,23 @@ __global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ Batc
   if (threadIdx.x == 0) s_carry = *J.count;
   __syncthreads();
   for (int chunk = 0; chunk < segs; chunk += 1024) {
+    // warp w counts segments chunk + 32 w .. + 31, one per step; lane k
+    // keeps the count of segment chunk + 32 w + k (= this thread's)
+    uint32_t v = 0u;
+    for (int k = 0; k < 32; ++k) {
+      const int si = chunk + warp * 32 + k;
+      uint32_t c = 0u;
+      if (si < segs) {
+        const int nw = seg_words(J, si);
+        const uint32_t* m = b.masks + static_cast<int64_t>(J.seg0 + si) * kWordsPerSeg;
+        c = (lane < nw ? __popc(m[lane]) : 0) + (lane + 32 < nw ? __popc(m[lane + 32]) : 0);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      if (lane == k) v = c;
+    }
     const int i = chunk + threadIdx.x;
-    const uint32_t v = i < segs ? b.counts[J.seg0 + i] : 0u;
+    if (i < segs) b.counts[J.seg0 + i] = v;
     uint32_t incl = v;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -271,7 +302,12 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(const __grid_constant__ 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int seg = blockIdx.x; seg < b.total_segs; seg += gridDim.x) {
     __syncthreads();
-    if (threadIdx.x < kWordsPerSeg) s_words[threadIdx.x] = b.masks[static_cast<int64_t>(seg) * kWordsPerSeg + threadIdx.x];
+    const Job& J = b.jobs[find_job(b, seg)];
+    const int local = seg - J.seg0;
+    if (threadIdx.x < kWordsPerSeg)
+      s_words[threadIdx.x] = static_cast<int>(threadIdx.x) < seg_words(J, local)
+                                 ? b.masks[static_cast<int64_t>(seg) * kWordsPerSeg + threadIdx.x]
+                                 : 0u;
     __syncthreads();
     if (threadIdx.x < 32) {
       const uint32_t a = __popc(s_words[2 * lane]), c = __popc(s_words[2 * lane + 1]);
@@ -286,8 +322,6 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(const __grid_constant__ 
       s_prefix[2 * lane + 1] = excl + a;
     }
     __syncthreads();
-    const Job& J = b.jobs[find_job(b, seg)];
-    const int local = seg - J.seg0;
     const int y = local / J.segs_per_row;
     const int x0 = (local % J.segs_per_row) * kSeg;
     const uint32_t base = b.offsets[seg];
@@ -331,8 +365,7 @@ int sm_count() {
 int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cudaStream_t s) {
   if (!jobs || n <= 0 || n > kMaxJobs) return HSI_E_INVALID;
   Batch b{};
-  int64_t segs = 0;
-  int max_r = 0;
+  int64_t segs = 0, tiles = 0;
   for (int i = 0; i < n; ++i) {
     const hsi_detect_job& j = jobs[i];
     if (!j.score || !j.count || j.height <= 0 || j.width <= 0 || j.capacity < 0) return HSI_E_INVALID;
@@ -351,30 +384,32 @@ int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cuda
     J.count = j.count;
     J.seg0 = static_cast<int>(segs);
     J.segs_per_row = (j.width + kSeg - 1) / kSeg;
+    J.tile0 = static_cast<int>(tiles);
+    J.tiles_x = (j.width + kTileW - 1) / kTileW;
     segs += segs_of(j.height, j.width);
-    // staged radii size the shared tile; larger ones read global memory
-    if (j.nms_radius <= kMaxStagedRadius && j.nms_radius > max_r) max_r = j.nms_radius;
+    tiles += static_cast<int64_t>(J.tiles_x) * ((j.height + kTileH - 1) / kTileH);
+    if (segs > 0x3fffffff || tiles > 0x3fffffff) return HSI_E_CAPACITY;
   }
-  if (segs > 0x3fffffff) return HSI_E_CAPACITY;
   if (!ws || ws_bytes < ws_bytes_for_segs(segs)) return HSI_E_WORKSPACE;
   if ((reinterpret_cast<uintptr_t>(ws) & 15u) != 0) return HSI_E_INVALID;
   b.njobs = n;
   b.total_segs = static_cast<int>(segs);
+  b.total_tiles = static_cast<int>(tiles);
   uint32_t* p = static_cast<uint32_t*>(ws);
   b.counts = p;
   b.offsets = p + segs;
   b.masks = p + 2 * segs;
-  const size_t smem = static_cast<size_t>(2 * (max_r > 0 ? max_r : 1) + 1) * (kSeg + 2 * max_r) * sizeof(float);
-  static bool configured = false;
-  if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute(flags_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>((2 * kMaxStagedRadius + 1) *
-                                                                (kSeg + 2 * kMaxStagedRadius) * sizeof(float)));
-    if (e != cudaSuccess) return static_cast<int>(e);
-    configured = true;
+  // one wave of resident tiles (30 KB of shared memory, 288 threads each)
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    int v = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, flags_kernel, kFlagThreads, 0) != cudaSuccess || v <= 0) v = 4;
+    per_sm = v;
   }
+  const int64_t wave = static_cast<int64_t>(per_sm) * sm_count();
+  const int flag_grid = static_cast<int>(tiles < wave ? tiles : wave);
   const int grid = static_cast<int>(segs < 16 * sm_count() ? segs : 16 * sm_count());
-  flags_kernel<<<grid, kThreads, smem, s>>>(b);
+  flags_kernel<<<flag_grid, kFlagThreads, 0, s>>>(b);
   scan_kernel<<<n, 1024, 0, s>>>(b);
   emit_kernel<<<grid, kThreads, 0, s>>>(b);
   return static_cast<int>(cudaGetLastError());
@@ -440,9 +475,10 @@ constexpr int kNoAllocSegs = HSI_DETECT_NOALLOC_MAX_SEGMENTS;
 constexpr size_t kNoAllocBytes = static_cast<size_t>(kNoAllocSegs) * sizeof(uint32_t) * (2 + kWordsPerSeg) + 256;
 
 // Segment counts, offsets and ballot masks of one call.  Every word a call
-// reads is written earlier by that same call (flags writes counts and all 64
-// mask words of each segment, scan writes offsets), so nothing here needs to
-// start at zero and stale contents from a previous call are never read.
+// reads is written earlier by that same call (flags writes every mask word
+// that covers pixels of the map, and scan and emit read no other; scan writes
+// the counts and offsets), so nothing here needs to start at zero and stale
+// contents from a previous call are never read.
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocBytes / sizeof(uint32_t)];
 
 constexpr int kNoAllocMaxDevices = 64;
@@ -450,8 +486,7 @@ std::mutex g_noalloc_mutex;
 void* g_noalloc_addr[kNoAllocMaxDevices];  // device address of the array, per device
 
 // Once per device, with that device current: look up the array's device
-// address (in host code its name is only a host-side stand-in) and allow the
-// flags kernel its full shared-memory tile on this device.
+// address (in host code its name is only a host-side stand-in).
 int noalloc_scratch(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -463,10 +498,6 @@ int noalloc_scratch(void** out) {
     e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
     if (e != cudaSuccess) return static_cast<int>(e);
     if ((reinterpret_cast<uintptr_t>(addr) & 255u) != 0) return HSI_E_INVALID;
-    e = cudaFuncSetAttribute(flags_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>((2 * kMaxStagedRadius + 1) * (kSeg + 2 * kMaxStagedRadius) *
-                                              sizeof(float)));
-    if (e != cudaSuccess) return static_cast<int>(e);
     g_noalloc_addr[dev] = addr;
   }
   *out = g_noalloc_addr[dev];

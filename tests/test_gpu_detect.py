@@ -45,8 +45,8 @@ def test_golden_hand_built_cases(hsi, golden):
     assert _tuples(d) == _tuples(golden["case_extremum_high"])
 
 
-@pytest.mark.parametrize("shape", [(1, 1), (1, 700), (700, 1), (37, 53), (256, 256), (1024, 2048)])
-@pytest.mark.parametrize("radius", [0, 1, 2, 4])
+@pytest.mark.parametrize("shape", [(1, 1), (1, 700), (700, 1), (37, 53), (256, 256), (130, 300), (1024, 2048)])
+@pytest.mark.parametrize("radius", [0, 1, 2, 4, 8, 11])
 @pytest.mark.parametrize("higher", [False, True])
 def test_random_plateaus_bit_exact(hsi, orc, shape, radius, higher):
     H, W = shape
@@ -64,9 +64,9 @@ def test_random_plateaus_bit_exact(hsi, orc, shape, radius, higher):
 @pytest.mark.parametrize("radius", [1, 3, 4])
 @pytest.mark.parametrize("higher", [False, True])
 def test_sparse_and_dense_segments_bit_exact(hsi, orc, radius, higher):
-    """Rows alternate between few candidates (their windows read from global
-    memory) and many (the staged window with the separable window-best), so
-    both suppression paths meet at shared window rows."""
+    """Rows alternate between few candidates and many, in a map three row
+    segments wide with a ragged last segment, so tiles see both densities
+    within one window."""
     H, W = 96, 4500
     rng = np.random.default_rng(1000 + radius)
     q = rng.integers(0, 50, (H, W)) / 50.0
