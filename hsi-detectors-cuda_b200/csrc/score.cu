@@ -35,14 +35,18 @@ constexpr int kFiltersPerPass = HSI_MAX_FILTERS_PER_PASS;
 template <typename T>
 struct CubeTraits;
 // Stage ring depth: with two consumer warpgroups two CTAs fit per SM, and
-// 12 stages per SM keep ~190 KB of each SM's reads in flight.
+// 12 stages per SM keep ~190 KB of each SM's reads in flight.  With both
+// banks in one warpgroup three CTAs fit (the warps hide the packed FMAs'
+// latency better), with 4 stages each for FP32.
 template <>
 struct CubeTraits<float> {
   static constexpr int kStages = 6;
+  static constexpr int kStagesFused = 4;
 };
 template <>
 struct CubeTraits<__half> {
   static constexpr int kStages = 10;
+  static constexpr int kStagesFused = 7;
 };
 
 struct ScoreParams {
@@ -105,17 +109,17 @@ struct SmemLayout {
 };
 
 template <typename T>
-__host__ __device__ inline SmemLayout smem_layout(int groups, int max_bands, int kg) {
+__host__ __device__ inline SmemLayout smem_layout(int groups, int max_bands, int slots, int stages) {
   SmemLayout l;
   l.stage_bytes = static_cast<size_t>(kStageBands) * kTile * sizeof(T);
-  size_t off = l.stage_bytes * CubeTraits<T>::kStages;
+  size_t off = l.stage_bytes * stages;
   l.filt_off = off;
-  off += static_cast<size_t>(groups) * max_bands * kg * 2 * sizeof(float);
+  off += static_cast<size_t>(groups) * max_bands * slots * sizeof(float);
   l.scale_off = off;
   off += static_cast<size_t>(groups) * kFiltersPerPass * sizeof(float);
   off = (off + 15) & ~static_cast<size_t>(15);
   l.bar_off = off;
-  off += 2 * CubeTraits<T>::kStages * sizeof(uint64_t);
+  off += 2 * static_cast<size_t>(stages) * sizeof(uint64_t);
   l.prefix_off = off;
   off += (kMaxTableFrames + 1) * sizeof(int) + 16;
   l.total = off;
@@ -202,15 +206,7 @@ __device__ __forceinline__ bool aligned16(const void* p) {
 // SAM epilogue for one thread's 4 pixels starting at frame pixel p.
 template <int KG>
 __device__ void sam_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, int valid,
-                             const float2 (&acc2)[KG][2], const float2 (&nrm2)[2], const float* scale) {
-  float acc[KG][kPPT], nrm[kPPT] = {nrm2[0].x, nrm2[0].y, nrm2[1].x, nrm2[1].y};
-#pragma unroll
-  for (int k = 0; k < KG; ++k) {
-    acc[k][0] = acc2[k][0].x;
-    acc[k][1] = acc2[k][0].y;
-    acc[k][2] = acc2[k][1].x;
-    acc[k][3] = acc2[k][1].y;
-  }
+                             const float (&acc)[KG][kPPT], const float (&nrm)[kPPT], const float* scale) {
   {
     const bool first = pass == 0;
     const bool last = pass_count(F.num_sam, pass + 1) == 0;
@@ -264,15 +260,7 @@ __device__ void sam_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, i
 
 template <int KG>
 __device__ void cem_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, int valid,
-                             const float2 (&acc2)[KG][2]) {
-  float acc[KG][kPPT];
-#pragma unroll
-  for (int k = 0; k < KG; ++k) {
-    acc[k][0] = acc2[k][0].x;
-    acc[k][1] = acc2[k][0].y;
-    acc[k][2] = acc2[k][1].x;
-    acc[k][3] = acc2[k][1].y;
-  }
+                             const float (&acc)[KG][kPPT]) {
   {
     const bool first = pass == 0;
     const int t0 = pass * kFiltersPerPass;
@@ -377,26 +365,189 @@ __device__ __forceinline__ void consumer_loop(const ScoreParams& prm, const int*
       const int64_t rem = P - p;
       const int valid = rem <= 0 ? 0 : (rem >= kPPT ? kPPT : static_cast<int>(rem));
       if (valid > 0) {
+        float a[KG][kPPT];
+#pragma unroll
+        for (int k = 0; k < KG; ++k) {
+          a[k][0] = acc[k][0].x;
+          a[k][1] = acc[k][0].y;
+          a[k][2] = acc[k][1].x;
+          a[k][3] = acc[k][1].y;
+        }
         if constexpr (kSam) {
-          sam_epilogue<KG>(F, prm.pass, n_f, p, valid, acc, nrm, scale);
+          const float n[kPPT] = {nrm[0].x, nrm[0].y, nrm[1].x, nrm[1].y};
+          sam_epilogue<KG>(F, prm.pass, n_f, p, valid, a, n, scale);
         } else {
-          cem_epilogue<KG>(F, prm.pass, n_f, p, valid, acc);
+          cem_epilogue<KG>(F, prm.pass, n_f, p, valid, a);
         }
       }
     }
   }
 }
 
+// Fused consumer: one warpgroup scores the SAM and the CEM bank together, so
+// each pixel leaves shared memory once for all KS + KC filters.  The bank is
+// stored band-major without duplication, [b][KS SAM | KC CEM]; accumulators
+// are filter pairs per pixel, (acc_k, acc_k+1) += (x, x) * (f_k, f_k+1), the
+// pixel duplicated in a register pair for the packed FMA.
+template <typename T, int K>
+__device__ __forceinline__ void consume_stage_fused(const T* stage, const float* filt, int nb, int tid,
+                                                    float2 (&acc)[K / 2][kPPT], float2 (&nrm)[2]) {
+  const T* src = stage + tid * kPPT;
+  auto band = [&](int i) {
+    float v[kPPT];
+    load4<T>(src + i * kTile, v);
+    const float2 v01 = make_float2(v[0], v[1]), v23 = make_float2(v[2], v[3]);
+    nrm[0] = ffma2(v01, v01, nrm[0]);
+    nrm[1] = ffma2(v23, v23, nrm[1]);
+    float2 d[kPPT];
+#pragma unroll
+    for (int j = 0; j < kPPT; ++j) d[j] = make_float2(v[j], v[j]);
+    const float* fr = filt + i * K;
+#pragma unroll
+    for (int k = 0; k < K; k += 4) {
+      const float4 f = ld_shared_f4(fr + k);  // (f_k, f_k+1, f_k+2, f_k+3)
+      const float2 fa = make_float2(f.x, f.y), fb = make_float2(f.z, f.w);
+#pragma unroll
+      for (int j = 0; j < kPPT; ++j) {
+        acc[k / 2][j] = ffma2(d[j], fa, acc[k / 2][j]);
+        acc[k / 2 + 1][j] = ffma2(d[j], fb, acc[k / 2 + 1][j]);
+      }
+    }
+  };
+  if (nb == kStageBands) {
+#pragma unroll
+    for (int i = 0; i < kStageBands; ++i) band(i);
+  } else {
+    for (int i = 0; i < nb; ++i) band(i);
+  }
+}
+
+template <typename T, int KS, int KC, int kStages>
+__device__ __forceinline__ void consumer_loop_fused(const ScoreParams& prm, const int* prefix, int total_tiles,
+                                                    unsigned char* smem, size_t stage_bytes, uint64_t* full,
+                                                    uint64_t* empty, volatile int* abort_flag, float* filt,
+                                                    float* scale, int tid, int lane) {
+  constexpr int K = KS + KC;
+  const int nframes = prm.num_frames;
+  int cur_frame = -1;
+  int n_s = 0, n_c = 0;
+  uint32_t it = 0;
+  bool aborted = false;
+  for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    const int f = find_frame(prefix, nframes, tile);
+    const hsi_frame& F = frame_at(prm, f);
+    const int B = F.bands;
+    if (f != cur_frame) {
+      named_sync(1, kGroupThreads);
+      n_s = pass_count(F.num_sam, prm.pass);
+      n_c = pass_count(F.num_cem, prm.pass);
+      const int t0 = prm.pass * kFiltersPerPass;
+      for (int i = tid; i < B * K; i += kGroupThreads) {
+        const int b = i / K, k = i % K;
+        float v = 0.0f;
+        if (k < KS) {
+          if (k < n_s) v = F.sam_targets[static_cast<int64_t>(t0 + k) * B + b];
+        } else if (k - KS < n_c) {
+          v = F.cem_weights[static_cast<int64_t>(t0 + k - KS) * B + b];
+        }
+        filt[i] = v;
+      }
+      if (tid < kFiltersPerPass) {
+        const float nrm = tid < n_s ? F.sam_norms[t0 + tid] : 0.0f;
+        scale[tid] = nrm > 0.0f ? 1.0f / nrm : 0.0f;
+      }
+      named_sync(1, kGroupThreads);
+      cur_frame = f;
+    }
+    const int64_t P = static_cast<int64_t>(F.height) * F.width;
+    const int64_t p0 = static_cast<int64_t>(tile - prefix[f]) * kTile;
+    const bool active = n_s > 0 || n_c > 0;
+
+    float2 acc[K / 2][kPPT];
+    float2 nrm[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+#pragma unroll
+    for (int k = 0; k < K / 2; ++k)
+#pragma unroll
+      for (int j = 0; j < kPPT; ++j) acc[k][j] = make_float2(0.0f, 0.0f);
+
+    for (int b0 = 0; b0 < B; b0 += kStageBands) {
+      const int nb = B - b0 < kStageBands ? B - b0 : kStageBands;
+      const int slot = static_cast<int>(it % kStages);
+      const uint32_t round = it / kStages;
+      if (!aborted && !mbar_wait(&full[slot], round & 1u)) {
+        record_error(prm.status, HSI_E_TIMEOUT);
+        *abort_flag = 1;
+        aborted = true;
+      }
+      if (active && !aborted) {
+        const T* stage = reinterpret_cast<const T*>(smem + slot * stage_bytes);
+        consume_stage_fused<T, K>(stage, filt + b0 * K, nb, tid, acc, nrm);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[slot]);
+      ++it;
+    }
+    if (active && !aborted) {
+      const int64_t p = p0 + tid * kPPT;
+      const int64_t rem = P - p;
+      const int valid = rem <= 0 ? 0 : (rem >= kPPT ? kPPT : static_cast<int>(rem));
+      if (valid > 0) {
+        if (n_s > 0) {
+          float a[KS][kPPT];
+#pragma unroll
+          for (int k = 0; k < KS; ++k)
+#pragma unroll
+            for (int j = 0; j < kPPT; ++j) a[k][j] = (k & 1) ? acc[k / 2][j].y : acc[k / 2][j].x;
+          const float n[kPPT] = {nrm[0].x, nrm[0].y, nrm[1].x, nrm[1].y};
+          sam_epilogue<KS>(F, prm.pass, n_s, p, valid, a, n, scale);
+        }
+        if (n_c > 0) {
+          float a[KC][kPPT];
+#pragma unroll
+          for (int k = 0; k < KC; ++k)
+#pragma unroll
+            for (int j = 0; j < kPPT; ++j)
+              a[k][j] = ((KS + k) & 1) ? acc[(KS + k) / 2][j].y : acc[(KS + k) / 2][j].x;
+          cem_epilogue<KC>(F, prm.pass, n_c, p, valid, a);
+        }
+      }
+    }
+  }
+}
+
+// Both banks in one warpgroup: 4 or 8 filters of each kind.
+template <int KS, int KC>
+constexpr bool fused_banks() {
+  return (KS == 4 || KS == 8) && (KC == 4 || KC == 8);
+}
+
 // Kernel: KS SAM filters and KC CEM filters per pass (0 = that warpgroup is
-// absent).  Block = (groups * 128 + 32) threads; the last warp produces.
+// absent; both in one warpgroup when fused_banks).  Block = (groups * 128 +
+// 32) threads; the last warp produces.
+template <int KS, int KC>
+constexpr int score_groups() {
+  return fused_banks<KS, KC>() ? 1 : (KS > 0) + (KC > 0);
+}
+// Filter slots per band per group in shared memory (duplicated pairs in the
+// two-group layout, plain in the fused one).
+template <int KS, int KC>
+constexpr int score_slots() {
+  return fused_banks<KS, KC>() ? KS + KC : 2 * (KS > KC ? KS : KC);
+}
+
 template <typename T, int KS, int KC>
-__global__ void __launch_bounds__(((KS > 0) + (KC > 0)) * kGroupThreads + 32)
+constexpr int score_stages() {
+  return fused_banks<KS, KC>() ? CubeTraits<T>::kStagesFused : CubeTraits<T>::kStages;
+}
+
+template <typename T, int KS, int KC>
+__global__ void __launch_bounds__(score_groups<KS, KC>() * kGroupThreads + 32, fused_banks<KS, KC>() ? 3 : 1)
     score_kernel(const __grid_constant__ ScoreParams prm, int max_bands) {
-  constexpr int kGroups = (KS > 0) + (KC > 0);
-  constexpr int kStages = CubeTraits<T>::kStages;
-  constexpr int kKG = (KS > KC ? KS : KC);  // filter slots per group in smem
+  constexpr int kGroups = score_groups<KS, KC>();
+  constexpr int kStages = score_stages<T, KS, KC>();
+  constexpr int kSlots = score_slots<KS, KC>();
   extern __shared__ __align__(128) unsigned char smem[];
-  const SmemLayout L = smem_layout<T>(kGroups, max_bands, kKG);
+  const SmemLayout L = smem_layout<T>(kGroups, max_bands, kSlots, kStages);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bar_off);
   uint64_t* empty = full + kStages;
   int* prefix = reinterpret_cast<int*>(smem + L.prefix_off);
@@ -480,8 +631,13 @@ __global__ void __launch_bounds__(((KS > 0) + (KC > 0)) * kGroupThreads + 32)
   // ---------------- consumer warpgroups ----------------
   const int group = warp / (kGroupThreads / 32);  // 0: SAM if KS > 0, else CEM; 1: CEM
   const int tid = threadIdx.x - group * kGroupThreads;
-  float* filt = reinterpret_cast<float*>(smem + L.filt_off) + static_cast<size_t>(group) * max_bands * kKG * 2;
+  float* filt = reinterpret_cast<float*>(smem + L.filt_off) + static_cast<size_t>(group) * max_bands * kSlots;
   float* scale = reinterpret_cast<float*>(smem + L.scale_off) + group * kFiltersPerPass;
+  if constexpr (fused_banks<KS, KC>()) {
+    consumer_loop_fused<T, KS, KC, kStages>(prm, prefix, total_tiles, smem, L.stage_bytes, full, empty, abort_flag,
+                                            filt, scale, tid, lane);
+    return;
+  }
   if constexpr (KS > 0) {
     if (group == 0) {
       consumer_loop<T, KS, true, kStages>(prm, prefix, total_tiles, smem, L.stage_bytes, full, empty,
@@ -520,9 +676,8 @@ int round_filters(int n) {
 
 template <typename T, int KS, int KC>
 int launch_instance(const ScoreParams& p, int max_bands, int ctas_per_sm, cudaStream_t stream) {
-  constexpr int kGroups = (KS > 0) + (KC > 0);
-  constexpr int kKG = (KS > KC ? KS : KC);
-  const SmemLayout L = smem_layout<T>(kGroups, max_bands, kKG);
+  constexpr int kGroups = score_groups<KS, KC>();
+  const SmemLayout L = smem_layout<T>(kGroups, max_bands, score_slots<KS, KC>(), score_stages<T, KS, KC>());
   const int threads = kGroups * kGroupThreads + 32;
   auto kernel = score_kernel<T, KS, KC>;
   static int configured_bytes = -1;

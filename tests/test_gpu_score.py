@@ -174,6 +174,50 @@ def test_cem_with_scene_statistics(hsi, orc, dtype):
     assert np.max(np.abs(r["cem_maps"] - all64)) < 1e-4
 
 
+@pytest.mark.parametrize("max_sam,max_cem", [(4, 4), (8, 8), (8, 4)])
+def test_sam_and_cem_banks_of_uneven_sizes(hsi, orc, max_sam, max_cem):
+    """One device table whose frames carry fewer filters than the launch
+    bounds (down to none of one kind): both banks are scored by one
+    warpgroup, and empty slots must neither score nor write."""
+    counts = [(max_sam, max_cem), (max_sam - 1, 0), (1, max_cem - 1), (0, max_cem)]
+    frames, keep = [], []
+    for i, (ns, nc) in enumerate(counts):
+        H, W, B = 40 + i, 48, 113 - 20 * i
+        sc = hsi.scene(B, n_targets=max(ns, nc, 1), target_frac=0.02, frame_seed=300 + i, library_seed=31 + i)
+        cube, _ = hsi.generate(sc, H, W)
+        lib = hsi.scene_targets(sc)
+        P = H * W
+        kw, out = {}, {}
+        if ns:
+            kw["sam_targets"] = torch.from_numpy(np.ascontiguousarray(lib[:ns])).cuda()
+            kw["sam_norms"] = torch.from_numpy(hsi.target_norms(lib[:ns])).cuda()
+            out["sam_best"] = torch.full((P,), -7.0, device="cuda")
+            out["sam_best_target"] = torch.full((P,), -7, dtype=torch.int32, device="cuda")
+            out["sam_maps"] = torch.full((ns, P), -7.0, device="cuda")
+        cem = None
+        if nc:
+            rng = np.random.default_rng(40 + i)
+            cem = (rng.standard_normal((nc, B)) / B).astype(np.float32)
+            kw["cem_weights"] = torch.from_numpy(cem).cuda()
+            out["cem_best"] = torch.full((P,), -7.0, device="cuda")
+            out["cem_best_target"] = torch.full((P,), -7, dtype=torch.int32, device="cuda")
+            out["cem_maps"] = torch.full((nc, P), -7.0, device="cuda")
+        frames.append(hsi.make_frame(cube, H, W, B, 0, map_stride=P, **kw, **out))
+        keep.append((cube, lib[:ns], cem, out, H, W, B, kw))
+    table = hsi.frame_table(frames)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    hsi.score_frames_device(table, len(frames), max_bands=113, max_sam=max_sam, max_cem=max_cem, status=status)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    for cube, targets, cem, out, H, W, B, _ in keep:
+        host = _download(cube, B, H * W)
+        r = {k: v.cpu().numpy() for k, v in out.items()}
+        if targets.shape[0]:
+            _check_sam(orc, host, targets, r["sam_best"], r["sam_best_target"], r["sam_maps"])
+        if cem is not None:
+            _check_cem(orc, host, cem, r)
+
+
 def test_batched_frames_inline_and_device_table(hsi, orc):
     shapes = [(30, 41, 113), (64, 32, 16), (17, 19, 224)]
     frames, keep = [], []
