@@ -427,6 +427,8 @@ def run_ours(args, workload):
                                                         [ms, kernel_ms, stats_ms, detect_ms], device)
     pixels_step = args.frames * H * W
     value = whole_job_mpix(world, pixels_step, ms)
+    # detections found per frame in the last step (the detection workload's density)
+    found = wl.counts.double().mean().item()
 
     # dominant kernel: the fused scoring pass
     peaks = {}
@@ -475,6 +477,7 @@ def run_ours(args, workload):
             "roofline": roofline,
             "roofline_stats": roofline_stats,
             "step_hbm_fraction": round(step_bytes / (ms / 1e3) / 1e9 / hbm, 4),
+            "detections_per_frame": round(found, 1),
             "step_split_ms": {"statistics": round(stats_ms, 3), "scoring": round(kernel_ms, 3),
                               "detection": round(detect_ms, 3)},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
@@ -485,10 +488,10 @@ def run_ours(args, workload):
 
 
 # DRAM bytes (read + write) per frame of the scoring kernel, from the ncu
-# captures summarised in profiles/ (score_kernel_samcem8_f32_1024x1024x113.md:
-# 2.219 GB for a 4-frame launch; rxace_tc_kernel_f32_2048x1024x113.md: one
+# captures summarised in profiles/ (score_kernel_samcem8_f32_4x1024x1024x113.md:
+# 2.250 GB for a 4-frame launch; rxace_tc_kernel_f32_2048x1024x113.md: one
 # frame).  The scorer's traffic grows with the frames in the launch.
-TRAFFIC_PER_FRAME = {"sam_cem": 554.63e6, "rx_ace": 1036.90e6}
+TRAFFIC_PER_FRAME = {"sam_cem": 562.52e6, "rx_ace": 1036.90e6}
 
 
 def load_traffic(workload, frames):
