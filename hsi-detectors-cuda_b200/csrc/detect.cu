@@ -39,7 +39,8 @@ constexpr int kTileW = 256;                        // columns per tile (8 ballot
 constexpr int kTileH = 64;                         // rows per tile
 constexpr int kMaxRingR = 8;                       // largest radius streamed through the ring
 constexpr int kAhead = 4;                          // rows in flight ahead of the window
-constexpr int kRing = 2 * kMaxRingR + 2 + kAhead;  // ring rows: window, one spare, rows in flight
+constexpr int kRing = 32;                          // ring rows (a power of two >= window + spare + in flight)
+static_assert(kRing >= 2 * kMaxRingR + 2 + kAhead, "ring too small for the window");
 constexpr int kRingCols = kTileW + 2 * kMaxRingR;  // 272
 constexpr int kFlagThreads = 288;                  // >= kRingCols, whole warps
 
@@ -127,13 +128,110 @@ __device__ bool local_best_global(const float* __restrict__ s, int x, int y, int
   return true;
 }
 
-__global__ void __launch_bounds__(kFlagThreads) flags_kernel(const __grid_constant__ Batch b) {
-  __shared__ float ring[kRing][kRingCols];  // score rows, NaN outside the frame
-  __shared__ float s_v[2][kRingCols];       // per column: first-best score of the window (two rows)
-  __shared__ int s_k[2][kRingCols];         //   its row within the window (0 .. 2r)
-  __shared__ float s_c[2][kRingCols];       //   the centre row's score
+// Shared memory of one flags tile.
+struct FlagsSmem {
+  float ring[kRing][kRingCols];   // score rows, NaN outside the frame
+  float2 best[2][kRingCols];      // per column: (first-best score of the window, its row 0 .. 2r as int bits)
+  float centre[2][kRingCols];     // per column: the centre row's score
+};
+
+// One tile whose window radius R is known at compile time (0 .. kMaxRingR).
+template <int R>
+__device__ __forceinline__ void flags_tile(const Batch& b, const Job& J, FlagsSmem& sm, int x0, int y0, int y1) {
+  constexpr int kCols = kTileW + 2 * R;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const float nan = __int_as_float(0x7fc00000);
+  const int W = J.width, H = J.height;
+  const bool higher = J.higher != 0;
+  const float thr = J.threshold;
+  const int cx = x0 - R + t;  // this thread's column in the vertical pass
+  const bool col_in = t < kCols && cx >= 0 && cx < W;
+  const int last = y1 - 1 + R;  // last row the tile reads
+  // One ring row per call: a 4-byte cp.async per in-frame column, NaN stored
+  // directly elsewhere, and one commit group per thread per call.
+  int next_row = y0 - R;
+  auto issue_next = [&]() {
+    if (next_row <= last && t < kCols) {
+      float* dst = &sm.ring[next_row & (kRing - 1)][t];
+      if (col_in && next_row >= 0 && next_row < H)
+        cp_async4(dst, J.score + static_cast<int64_t>(next_row) * W + cx);
+      else
+        *dst = nan;
+    }
+    cp_async_commit();
+    ++next_row;
+  };
+#pragma unroll
+  for (int k = 0; k < 2 * R + kAhead; ++k) issue_next();
+  for (int y = y0; y <= y1; ++y) {
+    // row y + R + kAhead reuses the slot of row y + R + kAhead - kRing, at
+    // most y - R - 2, whose last reader passed the previous barrier
+    if (y < y1) issue_next();
+    cp_async_wait<kAhead>();  // this thread's copies up to row y + R have landed
+    __syncthreads();          // ... and everyone's
+    if (y > y0 && t < kTileW) {
+      // candidates of row y - 1 against the column bests around them
+      const int yh = y - 1, hb = yh & 1;
+      const int x = x0 + t;
+      bool pass = false;
+      if (x < W) {
+        const float s = sm.centre[hb][t + R];
+        if (over_threshold(s, thr, higher)) {
+          pass = true;
+#pragma unroll
+          for (int dx = -R; dx <= R; ++dx) {
+            const float2 vk = sm.best[hb][t + R + dx];
+            const float v = vk.x;
+            const int k = __float_as_int(vk.y);
+            // first in the window's order: better score, or the same score
+            // at a lower linear index (an earlier row, or this row to the left)
+            if (!isnan(v) && (better(v, s, higher) || (v == s && (k < R || (k == R && dx < 0))))) pass = false;
+          }
+        }
+      }
+      const uint32_t word = __ballot_sync(0xffffffffu, pass);
+      if (lane == 0 && x0 + 32 * warp < W) *mask_word(b, J, yh, x0 + 32 * warp) = word;
+    }
+    if (y < y1 && t < kCols) {
+      // column t's first-best over rows y - R .. y + R
+      float bv = nan;
+      int bk = 0;
+#pragma unroll
+      for (int k = 0; k <= 2 * R; ++k) {
+        const float v = sm.ring[(y - R + k) & (kRing - 1)][t];
+        if (!isnan(v) && (isnan(bv) || better(v, bv, higher))) {
+          bv = v;
+          bk = k;
+        }
+        if (k == R) sm.centre[y & 1][t] = v;
+      }
+      sm.best[y & 1][t] = make_float2(bv, __int_as_float(bk));
+    }
+  }
+}
+
+// A tile whose radius is too large for the ring: each candidate's window
+// read from global memory.
+__device__ void flags_tile_global(const Batch& b, const Job& J, int x0, int y0, int y1) {
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int r = J.radius;
+  const bool higher = J.higher != 0;
+  for (int y = y0; y < y1; ++y) {
+    if (t >= kTileW) continue;
+    const int x = x0 + t;
+    bool pass = false;
+    if (x < J.width) {
+      const float s = J.score[static_cast<int64_t>(y) * J.width + x];
+      pass = over_threshold(s, J.threshold, higher) &&
+             local_best_global(J.score, x, y, J.width, J.height, r, s, higher);
+    }
+    const uint32_t word = __ballot_sync(0xffffffffu, pass);
+    if (lane == 0 && x0 + 32 * warp < J.width) *mask_word(b, J, y, x0 + 32 * warp) = word;
+  }
+}
+
+__global__ void __launch_bounds__(kFlagThreads) flags_kernel(const __grid_constant__ Batch b) {
+  __shared__ FlagsSmem sm;
   for (int tile = blockIdx.x; tile < b.total_tiles; tile += gridDim.x) {
     __syncthreads();  // the previous tile is done with the shared buffers
     const Job& J = b.jobs[find_job_tile(b, tile)];
@@ -141,93 +239,17 @@ __global__ void __launch_bounds__(kFlagThreads) flags_kernel(const __grid_consta
     const int x0 = (local % J.tiles_x) * kTileW;
     const int y0 = (local / J.tiles_x) * kTileH;
     const int y1 = min(J.height, y0 + kTileH);
-    const int W = J.width, H = J.height;
-    const bool higher = J.higher != 0;
-    const float thr = J.threshold;
-    const int r = J.radius > 0 ? J.radius : 0;
-    if (r > kMaxRingR) {
-      for (int y = y0; y < y1; ++y) {
-        if (t >= kTileW) continue;
-        const int x = x0 + t;
-        bool pass = false;
-        if (x < W) {
-          const float s = J.score[static_cast<int64_t>(y) * W + x];
-          pass = over_threshold(s, thr, higher) && local_best_global(J.score, x, y, W, H, r, s, higher);
-        }
-        const uint32_t word = __ballot_sync(0xffffffffu, pass);
-        if (lane == 0 && x0 + 32 * warp < W) *mask_word(b, J, y, x0 + 32 * warp) = word;
-      }
-      continue;
-    }
-    const int ncols = kTileW + 2 * r;
-    const int cx = x0 - r + t;  // this thread's column in the vertical pass
-    const bool col_in = t < ncols && cx >= 0 && cx < W;
-    const int last = y1 - 1 + r;  // last row the tile reads
-    // One ring row per call: a 4-byte cp.async per in-frame column, NaN
-    // stored directly elsewhere, and one commit group per thread per call.
-    int next_row = y0 - r, next_slot = 0;
-    auto issue_next = [&]() {
-      if (next_row <= last && t < ncols) {
-        float* dst = &ring[next_slot][t];
-        if (col_in && next_row >= 0 && next_row < H)
-          cp_async4(dst, J.score + static_cast<int64_t>(next_row) * W + cx);
-        else
-          *dst = nan;
-      }
-      cp_async_commit();
-      ++next_row;
-      next_slot = next_slot + 1 == kRing ? 0 : next_slot + 1;
-    };
-    for (int k = 0; k < 2 * r + kAhead; ++k) issue_next();
-    int top_slot = 0;  // ring slot of row y - r
-    for (int y = y0; y <= y1; ++y) {
-      // row y + r + kAhead reuses the slot of row y - r - 2 or older, whose
-      // last reader passed the barrier of the previous iteration
-      if (y < y1) issue_next();
-      cp_async_wait<kAhead>();  // this thread's copies up to row y + r have landed
-      __syncthreads();          // ... and everyone's
-      if (y > y0 && t < kTileW) {
-        // candidates of row y - 1 against the column bests around them
-        const int yh = y - 1, hb = yh & 1;
-        const int x = x0 + t;
-        bool pass = false;
-        if (x < W) {
-          const float s = s_c[hb][t + r];
-          if (over_threshold(s, thr, higher)) {
-            pass = true;
-            for (int dx = -r; dx <= r; ++dx) {
-              const float v = s_v[hb][t + r + dx];
-              const int k = s_k[hb][t + r + dx];
-              // first in the window's order: better score, or the same score
-              // at a lower linear index (an earlier row, or this row to the left)
-              if (!isnan(v) && (better(v, s, higher) || (v == s && (k < r || (k == r && dx < 0))))) {
-                pass = false;
-                break;
-              }
-            }
-          }
-        }
-        const uint32_t word = __ballot_sync(0xffffffffu, pass);
-        if (lane == 0 && x0 + 32 * warp < W) *mask_word(b, J, yh, x0 + 32 * warp) = word;
-      }
-      if (y < y1 && t < ncols) {
-        // column t's first-best over rows y - r .. y + r
-        float bv = nan;
-        int bk = 0;
-        int sl = top_slot;
-        for (int k = 0; k <= 2 * r; ++k) {
-          const float v = ring[sl][t];
-          if (!isnan(v) && (isnan(bv) || better(v, bv, higher))) {
-            bv = v;
-            bk = k;
-          }
-          if (k == r) s_c[y & 1][t] = v;
-          sl = sl + 1 == kRing ? 0 : sl + 1;
-        }
-        s_v[y & 1][t] = bv;
-        s_k[y & 1][t] = bk;
-      }
-      top_slot = top_slot + 1 == kRing ? 0 : top_slot + 1;
+    switch (J.radius > 0 ? J.radius : 0) {
+      case 0: flags_tile<0>(b, J, sm, x0, y0, y1); break;
+      case 1: flags_tile<1>(b, J, sm, x0, y0, y1); break;
+      case 2: flags_tile<2>(b, J, sm, x0, y0, y1); break;
+      case 3: flags_tile<3>(b, J, sm, x0, y0, y1); break;
+      case 4: flags_tile<4>(b, J, sm, x0, y0, y1); break;
+      case 5: flags_tile<5>(b, J, sm, x0, y0, y1); break;
+      case 6: flags_tile<6>(b, J, sm, x0, y0, y1); break;
+      case 7: flags_tile<7>(b, J, sm, x0, y0, y1); break;
+      case 8: flags_tile<8>(b, J, sm, x0, y0, y1); break;
+      default: flags_tile_global(b, J, x0, y0, y1); break;
     }
   }
 }
