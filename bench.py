@@ -265,8 +265,9 @@ class ClockSampler:
 class Workload:
     """Device-resident frames, libraries, outputs and the batched launch table."""
 
-    def __init__(self, hsi, torch, frames, workload, device, seed_base):
+    def __init__(self, hsi, torch, frames, workload, device, seed_base, dtype=0):
         self.hsi, self.torch, self.n, self.kind = hsi, torch, frames, workload
+        self.dtype = dtype  # 0: fp32 cubes, 1: fp16 cubes (accumulated in FP32)
         self.P = H * W
         self.stride = hsi.plane_stride(H, W)
         sc = hsi.scene(B, n_targets=TARGETS, target_frac=0.002, library_seed=0x5EED1000)
@@ -277,7 +278,7 @@ class Workload:
         for f in range(frames):
             s = hsi.scene(B, n_targets=TARGETS, target_frac=0.002, library_seed=0x5EED1000,
                           frame_seed=seed_base + f)
-            cube, _ = hsi.generate(s, H, W, truth=False, device=device)
+            cube, _ = hsi.generate(s, H, W, dtype=dtype, truth=False, device=device)
             self.cubes.append(cube)
         P = self.P
         self.sam_maps = torch.empty((frames, TARGETS, P), device=device)
@@ -301,7 +302,7 @@ class Workload:
             self.moments = torch.zeros((frames, B + B * B + 1), dtype=torch.float64, device=device)
             self.status = torch.zeros(frames, dtype=torch.int32, device=device)
             # every frame's moments in one batched launch sequence
-            jobs = [hsi.moments_job(self.cubes[f], H, W, B, self.moments[f], stride=self.stride)
+            jobs = [hsi.moments_job(self.cubes[f], H, W, B, self.moments[f], dtype=dtype, stride=self.stride)
                     for f in range(frames)]
             self.moment_jobs = (hsi.MomentsJob * frames)(*jobs)
             self.stats_bytes = hsi.lib().hsi_scene_moments_batch_workspace_bytes(self.moment_jobs, frames)
@@ -318,7 +319,7 @@ class Workload:
             if self.cem:
                 kw.update(cem_weights=self.cem_w[f], cem_maps=self.cem_maps[f], cem_best=self.cem_best[f],
                           cem_best_target=self.cem_bt[f])
-            frames.append(hsi.make_frame(cube, H, W, B, 0, **kw))
+            frames.append(hsi.make_frame(cube, H, W, B, self.dtype, **kw))
         return hsi.frame_table(frames)
 
     def step(self, stream, events=None):
@@ -342,7 +343,8 @@ class Workload:
             launches += 1
         if events is not None:
             events[0].record(stream)
-        hsi.score_frames_device(self.table, self.n, B, TARGETS, TARGETS if self.cem else 0, stream=stream)
+        hsi.score_frames_device(self.table, self.n, B, TARGETS, TARGETS if self.cem else 0, dtype=self.dtype,
+                                stream=stream)
         launches += 1
         if events is not None:
             events[1].record(stream)
@@ -358,10 +360,10 @@ class Workload:
     stats_launches = 9
 
 
-def algorithmic_bytes_score(frames, cem):
-    """Bytes the fused scoring pass must move: the cube once, every map and the
-    best/id outputs written once."""
-    per_px = 4 * B + 4 * TARGETS + 8
+def algorithmic_bytes_score(frames, cem, esize=4):
+    """Bytes the fused scoring pass must move: the cube once (esize bytes per
+    element), every map and the best/id outputs written once."""
+    per_px = esize * B + 4 * TARGETS + 8
     if cem:
         per_px += 4 * TARGETS + 8
     return frames * H * W * per_px
@@ -460,6 +462,35 @@ def run_ours(args, workload):
     del wl
     torch.cuda.empty_cache()
 
+    # the configuration's fp16 variant of the same frames (FP32 accumulation)
+    f16 = None
+    if workload in ("sam", "sam_cem"):
+        wl16 = Workload(hsi, torch, args.frames, workload, device, seed_base=rank_seed(0x5EED1000, rank), dtype=1)
+        for _ in range(args.warmup):
+            wl16.step(stream)
+        ev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(4)) for _ in range(args.steps)]
+        a16, b16 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        a16.record(stream)
+        for k in range(args.steps):
+            wl16.step(stream, ev[k])
+        b16.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms16 = a16.elapsed_time(b16) / args.steps
+        k16 = float(np.mean([e[0].elapsed_time(e[1]) for e in ev]))
+        s16 = float(np.mean([e[2].elapsed_time(e[0]) for e in ev]))
+        d16 = float(np.mean([e[1].elapsed_time(e[3]) for e in ev]))
+        ms16, k16, s16, d16 = max_over_ranks(dist if world > 1 else None, [ms16, k16, s16, d16], device)
+        ach16 = algorithmic_bytes_score(args.frames, wl16.cem, esize=2) / (k16 / 1e3) / 1e9
+        f16 = {"value": round(whole_job_mpix(world, pixels_step, ms16), 2), "unit": "Mpix/s",
+               "ms_per_step": round(ms16, 3), "dtype": "f16 storage, f32 accumulation",
+               "step_split_ms": {"statistics": round(s16, 3), "scoring": round(k16, 3), "detection": round(d16, 3)},
+               "scoring_roofline_frac": round(ach16 / hbm, 4)}
+        del wl16
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         times, threads, P = cpu_reference(workload, 128, 2)
@@ -482,6 +513,8 @@ def run_ours(args, workload):
                               "detection": round(detect_ms, 3)},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
         }
+        if f16 is not None:
+            line["f16_variant"] = f16
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
