@@ -320,6 +320,7 @@ class Workload:
                 kw.update(cem_weights=self.cem_w[f], cem_maps=self.cem_maps[f], cem_best=self.cem_best[f],
                           cem_best_target=self.cem_bt[f])
             frames.append(hsi.make_frame(cube, H, W, B, self.dtype, **kw))
+        self.frames = frames  # host descriptors for hsi_score_frames_batch
         return hsi.frame_table(frames)
 
     def step(self, stream, events=None):
@@ -343,8 +344,7 @@ class Workload:
             launches += 1
         if events is not None:
             events[0].record(stream)
-        hsi.score_frames_device(self.table, self.n, B, TARGETS, TARGETS if self.cem else 0, dtype=self.dtype,
-                                stream=stream)
+        hsi.score_frames_batch(self.frames, stream=stream)
         launches += 1
         if events is not None:
             events[1].record(stream)

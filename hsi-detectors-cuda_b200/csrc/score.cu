@@ -20,7 +20,9 @@
 // reduction src/detectors_cpu.cpp:158-187.
 #include <cuda_fp16.h>
 
-#include "common.cuh"
+#include <mutex>
+
+#include "tc.cuh"
 
 namespace hsi_b200 {
 namespace {
@@ -31,6 +33,7 @@ constexpr int kTile = kGroupThreads * kPPT;
 constexpr int kStageBands = 8;
 constexpr int kMaxTableFrames = 256;
 constexpr int kFiltersPerPass = HSI_MAX_FILTERS_PER_PASS;
+constexpr int kMaxInline = 64;  // frames whose descriptors travel inside one launch
 
 template <typename T>
 struct CubeTraits;
@@ -51,7 +54,7 @@ struct CubeTraits<__half> {
 
 struct ScoreParams {
   const hsi_frame* table;  // device descriptor table, or null for inline frames
-  hsi_frame inline_frames[HSI_MAX_INLINE_FRAMES];
+  hsi_frame inline_frames[kMaxInline];
   int num_frames;
   int pass;     // filters [16*pass, 16*pass + 16) of each kind
   int dtype;    // element type every frame of the launch must have
@@ -95,13 +98,12 @@ __device__ __forceinline__ void named_sync(int id, int threads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
 
-__device__ __forceinline__ int find_frame(const int* prefix, int n, int tile) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (prefix[mid] <= tile) lo = mid; else hi = mid - 1;
-  }
-  return lo;
+// Frame of a tile: the last f with prefix[f] <= tile (frames without tiles
+// are passed over).  A CTA walks its tiles in increasing order, so the search
+// starts at the frame of its previous tile and only moves forward.
+__device__ __forceinline__ int next_frame(const int* prefix, int n, int tile, int f) {
+  while (f + 1 < n && prefix[f + 1] <= tile) ++f;
+  return f;
 }
 
 struct SmemLayout {
@@ -312,8 +314,9 @@ __device__ __forceinline__ void consumer_loop(const ScoreParams& prm, const int*
   int n_f = 0;
   uint32_t it = 0;
   bool aborted = false;
+  int fcur = 0;  // tiles only move forward, and so does their frame
   for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-    const int f = find_frame(prefix, nframes, tile);
+    const int f = fcur = next_frame(prefix, nframes, tile, fcur);
     const hsi_frame& F = frame_at(prm, f);
     const int B = F.bands;
     if (f != cur_frame) {
@@ -433,8 +436,9 @@ __device__ __forceinline__ void consumer_loop_fused(const ScoreParams& prm, cons
   int n_s = 0, n_c = 0;
   uint32_t it = 0;
   bool aborted = false;
+  int fcur = 0;  // tiles only move forward, and so does their frame
   for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-    const int f = find_frame(prefix, nframes, tile);
+    const int f = fcur = next_frame(prefix, nframes, tile, fcur);
     const hsi_frame& F = frame_at(prm, f);
     const int B = F.bands;
     if (f != cur_frame) {
@@ -593,8 +597,9 @@ __global__ void __launch_bounds__(score_groups<KS, KC>() * kGroupThreads + 32, f
       bool aborted = false;
       uint32_t pending = 0;         // bit s: slot s has copies issued
       uint32_t pending_parity = 0;  // bit s: phase parity of that issue
+      int fcur = 0;  // tiles only move forward, and so does their frame
       for (int tile = blockIdx.x; tile < total_tiles && !aborted; tile += gridDim.x) {
-        const int f = find_frame(prefix, nframes, tile);
+        const int f = fcur = next_frame(prefix, nframes, tile, fcur);
         const hsi_frame& F = frame_at(prm, f);
         const int64_t P = static_cast<int64_t>(F.height) * F.width;
         const int64_t p0 = static_cast<int64_t>(tile - prefix[f]) * kTile;
@@ -648,6 +653,486 @@ __global__ void __launch_bounds__(score_groups<KS, KC>() * kGroupThreads + 32, f
   if constexpr (KC > 0) {
     consumer_loop<T, KC, false, kStages>(prm, prefix, total_tiles, smem, L.stage_bytes, full, empty,
                                          abort_flag, filt, scale, group, tid, lane);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core scorer for FP16 cubes of at most 128 bands (kind::f16 MMAs).
+//
+// An FP16 cube value is an exact f16 MMA operand, and a TMA box of 64 pixels x
+// Bp bands loaded with the 128-byte swizzle is already the MN-major operand
+// layout, so the cube goes from HBM to the tensor cores with no conversion
+// pass.  Each filter f (a SAM target or CEM weight vector, FP32) is scaled by
+// a power of two 2^s (its largest |weight| to [0.5, 1)) and split into an f16
+// head fh = rn(f 2^s) and remainder fl = rn(f 2^s - fh), 22 significant bits
+// together.  B stacks the heads over the remainders (N2 = 2 N rows), so one
+// MMA per 16 bands gives x.fh and x.fl in separate TMEM columns, and
+// x.f = (x.fh + x.fl) 2^-s in the epilogue.  Products are exact, sums FP32.
+//
+// Per 128-pixel tile, one CTA per SM:
+//   warp 0       producer: two TMA boxes (64 px x Bp bands, 128-byte swizzle)
+//   warp 1       TMEM allocator + MMA issuer: Bp / 16 MMAs (M 128, N N2, K 16)
+//                into one of four accumulators
+//   warps 2-5    readers: the pixels' squared norms (SAM) from each stage, and
+//                the filter bank (heads, remainders, multipliers) at frame changes
+//   warps 6-21   epilogue, two teams of eight warps taking alternate tiles (four
+//                SAM, four CEM warps each; one pixel per thread): the angle /
+//                response / best-target rules of the FP32 scorer.  Two teams
+//                put two epilogue warps of a kind on each SM sub-partition, so
+//                the per-pixel arccosines and stores of one hide the latency of
+//                the other's.
+// ---------------------------------------------------------------------------
+constexpr int kHTile = 128;
+constexpr int kHStages = 6;
+constexpr int kHMaxBands = 128;
+constexpr int kHAcc = 4;  // TMEM accumulators (and norm buffers) in flight
+constexpr int kHThreads = 22 * 32;
+
+struct HSmem {
+  size_t stage_bytes, in_off, filt_off, norm_off, scale_off, bar_off, slot_off, total;
+};
+
+// bp: bands rounded up to 16; n2: rows of B (heads and remainders).
+__host__ __device__ inline HSmem h_smem(int bp, int n2) {
+  HSmem s;
+  s.stage_bytes = static_cast<size_t>(2) * bp * 128;  // two 64-pixel boxes
+  size_t off = 0;
+  s.in_off = off;  // 1024-aligned stages (bp * 128 is a multiple of 2048)
+  off += kHStages * s.stage_bytes;
+  s.filt_off = off;  // K-major, 64 bands per 128-byte row: (bp / 64 rounded up) chunks of n2 rows
+  off += static_cast<size_t>((bp + 63) / 64) * n2 * 128;
+  s.norm_off = off;  // [kHAcc buffers][4 reader warps][128 px]
+  off += kHAcc * 4 * kHTile * sizeof(float);
+  s.scale_off = off;  // [2 epochs][32 filters]
+  off += 2 * 32 * sizeof(float);
+  s.bar_off = off;
+  off += (2 * kHStages + 4 * kHAcc + 2 + 2 * 2 + 1) * sizeof(uint64_t);
+  s.slot_off = off;
+  off += 16;
+  s.total = off + 1024;
+  return s;
+}
+
+// Launch parameters: descriptors and tensor maps of up to 64 FP16 frames.
+struct HParams {
+  CUtensorMap maps[kMaxInline];
+  hsi_frame frames[kMaxInline];
+  int num_frames;
+  int pass;
+  int max_sam, max_cem;
+  int bp;       // bands of every frame rounded up to 16, at most 128
+  int* status;  // nullable device error word
+};
+
+// KS SAM and KC CEM filters per pass (each 0, 8 or 16); N = KS + KC rounded
+// up to 16, N2 = 2 N.
+template <int KS, int KC>
+__global__ void __launch_bounds__(kHThreads, 1) score_h_kernel(const __grid_constant__ HParams prm) {
+  constexpr int N = (KS + KC + 15) / 16 * 16;
+  constexpr int N2 = 2 * N;
+  constexpr uint32_t kCols = kHAcc * N2;  // 128 or 256 TMEM columns
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int bp = prm.bp;
+  const HSmem L = h_smem(bp, N2);
+  uint64_t* in_full = reinterpret_cast<uint64_t*>(smem + L.bar_off);
+  uint64_t* in_empty = in_full + kHStages;
+  uint64_t* acc_full = in_empty + kHStages;
+  uint64_t* acc_empty = acc_full + kHAcc;
+  uint64_t* norm_full = acc_empty + kHAcc;
+  uint64_t* norm_empty = norm_full + kHAcc;
+  uint64_t* filt_full = norm_empty + kHAcc;  // readers -> MMA: the bank of the new frame is in place
+  uint64_t* filt_free = filt_full + 1;    // MMA -> readers: every MMA on the old bank has completed
+  uint64_t* sc_full = filt_free + 1;      // readers -> epilogue: scales of epoch e & 1
+  uint64_t* sc_empty = sc_full + 2;       // epilogue -> readers
+  uint64_t* mma_done = sc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.slot_off);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.slot_off + 8);
+  __shared__ int prefix[kMaxInline + 1];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nframes = prm.num_frames;
+  for (int f = threadIdx.x; f < nframes; f += blockDim.x) {
+    const hsi_frame& F = prm.frames[f];
+    const int64_t P = static_cast<int64_t>(F.height) * F.width;
+    const bool ok = F.bands > 0 && F.bands <= bp && F.num_sam >= 0 && F.num_sam <= prm.max_sam && F.num_cem >= 0 &&
+                    F.num_cem <= prm.max_cem && F.dtype == HSI_F16 && P > 0 && F.plane_stride >= P &&
+                    (F.plane_stride & 7) == 0;
+    if (!ok && blockIdx.x == 0) record_error(prm.status, HSI_E_INVALID);
+    const bool any = ok && (pass_count(F.num_sam, prm.pass) > 0 || pass_count(F.num_cem, prm.pass) > 0);
+    prefix[f + 1] = any ? static_cast<int>(div_up<int64_t>(P, kHTile)) : 0;
+  }
+  if (threadIdx.x == 0) {
+    prefix[0] = 0;
+    *abort_flag = 0;
+    for (int s = 0; s < kHStages; ++s) {
+      mbar_init(&in_full[s], 1);
+      mbar_init(&in_empty[s], 1 + 4);  // the MMA commit and the four reader warps
+    }
+    for (int s = 0; s < kHAcc; ++s) {
+      mbar_init(&acc_full[s], 1);
+      mbar_init(&acc_empty[s], 8);   // the eight warps of the team that takes the tile
+      mbar_init(&norm_full[s], 4);
+      mbar_init(&norm_empty[s], 4);  // that team's SAM warps
+    }
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&sc_full[s], 4);
+      mbar_init(&sc_empty[s], 16);  // every epilogue warp
+    }
+    mbar_init(filt_full, 4);
+    mbar_init(filt_free, 1);
+    mbar_init(mma_done, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, kCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x == 0)
+    for (int f = 0; f < nframes; ++f) prefix[f + 1] += prefix[f];
+  __syncthreads();
+  const int total_tiles = prefix[nframes];
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t box_bytes = static_cast<uint32_t>(bp) * 128;
+
+  if (warp == 0) {
+    // ---------------- producer ----------------
+    if (lane == 0) {
+      uint32_t it = 0, pending = 0, parity = 0;
+      int fcur = 0;  // tiles only move forward, and so does their frame
+      for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++it) {
+        const int f = fcur = next_frame(prefix, nframes, tile, fcur);
+        const int x0 = (tile - prefix[f]) * kHTile;
+        const int s = it % kHStages;
+        const uint32_t ph = (it / kHStages) & 1u;
+        if (*abort_flag || !mbar_wait(&in_empty[s], ph ^ 1u)) {
+          record_error(prm.status, HSI_E_TIMEOUT);
+          *abort_flag = 1;
+          break;
+        }
+        unsigned char* dst = smem + L.in_off + static_cast<size_t>(s) * L.stage_bytes;
+        mbar_arrive_expect_tx(&in_full[s], 2 * box_bytes);
+        tma_load_2d(dst, &prm.maps[f], x0, 0, &in_full[s]);
+        tma_load_2d(dst + box_bytes, &prm.maps[f], x0 + 64, 0, &in_full[s]);
+        pending |= 1u << s;
+        parity = (parity & ~(1u << s)) | (ph << s);
+      }
+      // never leave copies in flight into this CTA's shared memory
+      for (int s = 0; s < kHStages; ++s)
+        if ((pending >> s) & 1u) mbar_wait(&in_full[s], (parity >> s) & 1u);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      const uint32_t idesc = idesc_f16_amn(kHTile, N2);
+      const unsigned char* filt = smem + L.filt_off;
+      uint32_t it = 0, epoch = 0;
+      int cur = -1;
+      bool ok = true, issued = false;
+      int fcur = 0;  // tiles only move forward, and so does their frame
+      for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x, ++it) {
+        const int f = fcur = next_frame(prefix, nframes, tile, fcur);
+        if (f != cur) {
+          // hand the bank back once every MMA on it has completed, then wait
+          // for the new one
+          if (cur >= 0) umma_commit(filt_free);
+          if (*abort_flag || !mbar_wait(filt_full, epoch & 1u)) {
+            record_error(prm.status, HSI_E_TIMEOUT);
+            *abort_flag = 1;
+            break;
+          }
+          tc_fence_after();
+          cur = f;
+          ++epoch;
+        }
+        const int s = it % kHStages, buf = it % kHAcc;
+        if (!mbar_wait(&in_full[s], (it / kHStages) & 1u) || !mbar_wait(&acc_empty[buf], ((it / kHAcc) & 1u) ^ 1u)) {
+          record_error(prm.status, HSI_E_TIMEOUT);
+          *abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const unsigned char* a = smem + L.in_off + static_cast<size_t>(s) * L.stage_bytes;
+        const int ksteps = div_up(prm.frames[f].bands, 16);
+        for (int ks = 0; ks < ksteps; ++ks) {
+          const uint64_t da = smem_desc_mn_sw128(a + ks * 2048, box_bytes);
+          const uint64_t db = smem_desc_sw128(filt + (ks >> 2) * N2 * 128) + 2 * (ks & 3);
+          umma_f16(tmem + buf * N2, da, db, idesc, ks > 0 ? 1u : 0u);
+        }
+        umma_commit(&in_empty[s]);
+        umma_commit(&acc_full[buf]);
+        issued = true;
+      }
+      if (issued) {
+        umma_commit(mma_done);
+        if (!mbar_wait(mma_done, 0)) record_error(prm.status, HSI_E_TIMEOUT);
+      }
+    }
+  } else if (warp < 6) {
+    // ---------------- readers: squared norms and the filter bank ----------------
+    const int rt = threadIdx.x - 64;        // 0..127
+    const int ch = rt & 15, bg = rt >> 4;   // pixels 8 ch .. 8 ch + 7; bands bg, bg + 8, ...
+    const int rw = warp - 2;                // reader warp 0..3
+    uint32_t it = 0, epoch = 0;
+    int cur = -1;
+    bool ok = true;
+    int fcur = 0;  // tiles only move forward, and so does their frame
+    for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x, ++it) {
+      const int f = fcur = next_frame(prefix, nframes, tile, fcur);
+      const hsi_frame& F = prm.frames[f];
+      if (f != cur) {
+        if (epoch > 0 && !mbar_wait(filt_free, (epoch - 1) & 1u)) {
+          ok = false;
+          break;
+        }
+        if (!mbar_wait(&sc_empty[epoch & 1u], ((epoch >> 1) & 1u) ^ 1u)) {
+          ok = false;
+          break;
+        }
+        // filter n: heads in row n, remainders in row N + n; bp / 8 threads per filter... here
+        // 128 / N threads per filter, each over every (128 / N)-th band
+        const int tpf = 128 / N, n = rt / tpf, j0 = rt % tpf;
+        const int n_s = pass_count(F.num_sam, prm.pass), n_c = pass_count(F.num_cem, prm.pass);
+        const int t0 = prm.pass * kFiltersPerPass;
+        const float* src = nullptr;
+        if (n < KS) {
+          if (n < n_s) src = F.sam_targets + static_cast<int64_t>(t0 + n) * F.bands;
+        } else if (n - KS < KC && n - KS < n_c) {
+          src = F.cem_weights + static_cast<int64_t>(t0 + n - KS) * F.bands;
+        }
+        float mx = 0.0f;
+        for (int b = j0; b < F.bands; b += tpf)
+          if (src) mx = fmaxf(mx, fabsf(src[b]));
+        for (int o = tpf / 2; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        int e2 = 0;
+        if (mx > 0.0f) frexpf(mx, &e2);  // mx in [2^(e2-1), 2^e2)
+        const float up = ldexpf(1.0f, -e2);
+        unsigned char* filt = smem + L.filt_off;
+        for (int b = j0; b < bp; b += tpf) {
+          const float v = (src && b < F.bands) ? src[b] * up : 0.0f;
+          const __half h = __float2half_rn(v);
+          const __half l = __float2half_rn(v - __half2float(h));
+          const int k2 = (b & 63) * 2;
+          const uint32_t row_h = static_cast<uint32_t>(n), row_l = static_cast<uint32_t>(N + n);
+          const uint32_t base = static_cast<uint32_t>((b >> 6) * N2 * 128);
+          const uint32_t oh = base + (row_h >> 3) * 1024 + (row_h & 7) * 128 + ((((k2 >> 4) ^ (row_h & 7))) << 4) + (k2 & 15);
+          const uint32_t ol = base + (row_l >> 3) * 1024 + (row_l & 7) * 128 + ((((k2 >> 4) ^ (row_l & 7))) << 4) + (k2 & 15);
+          *reinterpret_cast<__half*>(filt + oh) = h;
+          *reinterpret_cast<__half*>(filt + ol) = l;
+        }
+        // multiplier of column pair n: x.f = (x.fh + x.fl) 2^e2, and SAM folds in 1 / |r_t|
+        float mult = ldexpf(1.0f, e2);
+        if (n < KS) {
+          const float nr = n < n_s ? F.sam_norms[t0 + n] : 0.0f;
+          mult = nr > 0.0f ? mult / nr : 0.0f;
+        }
+        float* sc = reinterpret_cast<float*>(smem + L.scale_off) + (epoch & 1u) * 32;
+        if (j0 == 0) sc[n] = mult;
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(filt_full);
+          mbar_arrive(&sc_full[epoch & 1u]);
+        }
+        cur = f;
+        ++epoch;
+      }
+      // squared norms of the tile's pixels
+      const int s = it % kHStages, nb = it % kHAcc;
+      if (!mbar_wait(&in_full[s], (it / kHStages) & 1u) || !mbar_wait(&norm_empty[nb], ((it / kHAcc) & 1u) ^ 1u)) {
+        ok = false;
+        break;
+      }
+      const unsigned char* st = smem + L.in_off + static_cast<size_t>(s) * L.stage_bytes;
+      const int box = ch >> 3, c = ch & 7;  // 64-pixel box, 16-byte chunk (8 px) of its 128-byte rows
+      float2 acc[4] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f),
+                       make_float2(0.0f, 0.0f)};
+      // rows from the frame's band count up to bp are the box's zero fill, so
+      // every thread runs bp / 16 iterations of two bands (b, b + 8), loads first
+      const unsigned char* col = st + box * box_bytes + ((c ^ (bg & 7)) << 4) + bg * 128;
+#pragma unroll 4
+      for (int b = 0; b < bp; b += 16) {
+        // (b + bg) & 7 == bg & 7: the swizzled chunk is the same in every row this thread reads
+        const uint4 r0 = *reinterpret_cast<const uint4*>(col + b * 128);
+        const uint4 r1 = *reinterpret_cast<const uint4*>(col + b * 128 + 1024);
+        const __half2* h0 = reinterpret_cast<const __half2*>(&r0);
+        const __half2* h1 = reinterpret_cast<const __half2*>(&r1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float2 v0 = __half22float2(h0[q]);
+          const float2 v1 = __half22float2(h1[q]);
+          acc[q] = ffma2(v0, v0, acc[q]);
+          acc[q] = ffma2(v1, v1, acc[q]);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&in_empty[s]);
+      // two band groups per warp (lanes 16 apart), then one partial per reader warp
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        acc[q].x += __shfl_xor_sync(0xffffffffu, acc[q].x, 16);
+        acc[q].y += __shfl_xor_sync(0xffffffffu, acc[q].y, 16);
+      }
+      float* out = reinterpret_cast<float*>(smem + L.norm_off) + (nb * 4 + rw) * kHTile + 8 * ch;
+      if (lane < 16) {
+        *reinterpret_cast<float4*>(out) = make_float4(acc[0].x, acc[0].y, acc[1].x, acc[1].y);
+        *reinterpret_cast<float4*>(out + 4) = make_float4(acc[2].x, acc[2].y, acc[3].x, acc[3].y);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&norm_full[nb]);
+    }
+    if (!ok) {
+      record_error(prm.status, HSI_E_TIMEOUT);
+      *abort_flag = 1;
+    }
+  } else {
+    // ---------------- epilogue ----------------
+    const int team = (warp - 6) >> 3;            // takes the tiles with it % 2 == team
+    const bool cem = ((warp - 6) & 7) >= 4;
+    const int quarter = warp & 3;  // TMEM lane quarter of this warp
+    const int m = quarter * 32 + lane;
+    const uint32_t tq = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
+    uint32_t it = 0, epoch = 0;
+    int cur = -1;
+    float scale[16];  // multipliers of this warp's filters (SAM or CEM) for the current frame
+    int fcur = 0;  // tiles only move forward, and so does their frame
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++it) {
+      const int f = fcur = next_frame(prefix, nframes, tile, fcur);
+      const hsi_frame& F = prm.frames[f];
+      if (f != cur) {
+        if (*abort_flag || !mbar_wait(&sc_full[epoch & 1u], (epoch >> 1) & 1u)) {
+          record_error(prm.status, HSI_E_TIMEOUT);
+          *abort_flag = 1;
+          break;
+        }
+        const float* sc = reinterpret_cast<const float*>(smem + L.scale_off) + (epoch & 1u) * 32 + (cem ? KS : 0);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) scale[k] = sc[k];
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sc_empty[epoch & 1u]);
+        cur = f;
+        ++epoch;
+      }
+      if (static_cast<int>(it & 1u) != team) continue;
+      const int buf = it % kHAcc;
+      if (*abort_flag || !mbar_wait(&acc_full[buf], (it / kHAcc) & 1u) ||
+          (!cem && !mbar_wait(&norm_full[buf], (it / kHAcc) & 1u))) {
+        record_error(prm.status, HSI_E_TIMEOUT);
+        *abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const int64_t P = static_cast<int64_t>(F.height) * F.width;
+      const int64_t p = static_cast<int64_t>(tile - prefix[f]) * kHTile + m;
+      const bool in_frame = p < P;
+      const uint32_t d0 = tq + buf * N2;
+      const int t0 = prm.pass * kFiltersPerPass;
+      // filters c .. c+7 of this kind: (head + remainder columns) x multiplier
+      auto dots8 = [&](int c, float (&dot)[8]) {
+        uint32_t h[8], l[8];
+        const int col = (cem ? KS : 0) + c;
+        tmem_ld8(d0 + col, h);
+        tmem_ld8(d0 + N + col, l);
+        tmem_wait_ld();
+#pragma unroll
+        for (int k = 0; k < 8; ++k) dot[k] = (__uint_as_float(h[k]) + __uint_as_float(l[k])) * scale[c + k];
+      };
+      if (!cem) {
+        if constexpr (KS > 0) {
+          const int n_s = pass_count(F.num_sam, prm.pass);
+          const float* nrm_in = reinterpret_cast<const float*>(smem + L.norm_off) + buf * 4 * kHTile + m;
+          const float nrm = (nrm_in[0] + nrm_in[kHTile]) + (nrm_in[2 * kHTile] + nrm_in[3 * kHTile]);
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&norm_empty[buf]);
+          if (n_s > 0) {
+            const float rn = nrm > 0.0f ? rsqrtf(nrm) : 0.0f;
+            const bool last = pass_count(F.num_sam, prm.pass + 1) == 0;
+            float best = -2.0f;
+            int32_t best_t = -1;
+            if (prm.pass != 0 && in_frame) {
+              if (F.sam_best) best = F.sam_best[p];
+              if (F.sam_best_target) best_t = F.sam_best_target[p];
+            }
+            float cs[KS];
+#pragma unroll
+            for (int c = 0; c < KS; c += 8) {
+              float dot[8];
+              dots8(c, dot);
+#pragma unroll
+              for (int k = 0; k < 8; ++k) cs[c + k] = dot[k] * rn;
+            }
+#pragma unroll
+            for (int k = 0; k < KS; ++k)
+              if (k < n_s && cs[k] > best) {
+                best = cs[k];
+                best_t = t0 + k;
+              }
+            if (F.sam_maps && in_frame) {
+              float* const maps = F.sam_maps + static_cast<int64_t>(t0) * F.map_stride + p;
+              float ang[KS];
+#pragma unroll
+              for (int k = 0; k < KS; ++k) ang[k] = angle_of_cos(cs[k]);
+#pragma unroll
+              for (int k = 0; k < KS; ++k)
+                if (k < n_s) maps[k * F.map_stride] = ang[k];
+            }
+            if (in_frame) {
+              if (F.sam_best) F.sam_best[p] = last ? angle_of_cos(best) : best;
+              if (F.sam_best_target) F.sam_best_target[p] = best_t;
+            }
+          }
+        } else {
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&norm_empty[buf]);
+        }
+      } else {
+        if constexpr (KC > 0) {
+          const int n_c = pass_count(F.num_cem, prm.pass);
+          if (n_c > 0) {
+            float best = -INFINITY;
+            int32_t best_t = -1;
+            if (prm.pass != 0 && in_frame) {
+              if (F.cem_best) best = F.cem_best[p];
+              if (F.cem_best_target) best_t = F.cem_best_target[p];
+            }
+            float r[KC];
+#pragma unroll
+            for (int c = 0; c < KC; c += 8) {
+              float dot[8];
+              dots8(c, dot);
+#pragma unroll
+              for (int k = 0; k < 8; ++k) r[c + k] = dot[k];
+            }
+#pragma unroll
+            for (int k = 0; k < KC; ++k)
+              if (k < n_c && r[k] > best) {
+                best = r[k];
+                best_t = t0 + k;
+              }
+            if (F.cem_maps && in_frame) {
+              float* const maps = F.cem_maps + static_cast<int64_t>(t0) * F.map_stride + p;
+#pragma unroll
+              for (int k = 0; k < KC; ++k)
+                if (k < n_c) maps[k * F.map_stride] = r[k];
+            }
+            if (in_frame) {
+              if (F.cem_best) F.cem_best[p] = best;
+              if (F.cem_best_target) F.cem_best_target[p] = best_t;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[buf]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, kCols);
   }
 }
 
@@ -759,29 +1244,143 @@ int run_passes(ScoreParams& p, int dtype, int max_bands, int max_sam, int max_ce
   return HSI_OK;
 }
 
+template <int KS, int KC>
+int launch_h(const HParams& p, cudaStream_t stream) {
+  constexpr int N2 = 2 * ((KS + KC + 15) / 16 * 16);
+  auto kernel = score_h_kernel<KS, KC>;
+  const HSmem L = h_smem(p.bp, N2);
+  static int configured = -1;
+  if (configured < static_cast<int>(L.total)) {
+    const HSmem big = h_smem(kHMaxBands, N2);
+    const cudaError_t e =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(big.total));
+    if (e != cudaSuccess) return static_cast<int>(e);
+    configured = static_cast<int>(big.total);
+  }
+  kernel<<<sm_count(), kHThreads, L.total, stream>>>(p);
+  return static_cast<int>(cudaGetLastError());
+}
+
+// Tensor-core filter counts per kind: 0, 8 or 16.
+int round_h(int n) { return n == 0 ? 0 : (n <= 8 ? 8 : 16); }
+
+int dispatch_h(int ks, int kc, const HParams& p, cudaStream_t s) {
+  switch (ks * 100 + kc) {
+    case 8: return launch_h<0, 8>(p, s);
+    case 16: return launch_h<0, 16>(p, s);
+    case 800: return launch_h<8, 0>(p, s);
+    case 808: return launch_h<8, 8>(p, s);
+    case 816: return launch_h<8, 16>(p, s);
+    case 1600: return launch_h<16, 0>(p, s);
+    case 1608: return launch_h<16, 8>(p, s);
+    case 1616: return launch_h<16, 16>(p, s);
+    default: return HSI_E_INVALID;
+  }
+}
+
+bool tensor_core_frame(const hsi_frame& f) { return f.dtype == HSI_F16 && f.bands <= kHMaxBands; }
+
+// Tensor-core scorer over up to 64 validated FP16 frames: a 2-D tensor map
+// (128-byte swizzle, boxes of 64 pixels x all bands) per cube, one launch per
+// pass.
+int score_h_group(const hsi_frame* const* frames, int n, int* status, cudaStream_t s) {
+  static HParams p;  // 16 KB: kept off the stack; the launch copies it
+  p = HParams{};
+  p.num_frames = n;
+  p.status = status;
+  int max_bands = 0;
+  for (int i = 0; i < n; ++i) {
+    max_bands = frames[i]->bands > max_bands ? frames[i]->bands : max_bands;
+    p.max_sam = frames[i]->num_sam > p.max_sam ? frames[i]->num_sam : p.max_sam;
+    p.max_cem = frames[i]->num_cem > p.max_cem ? frames[i]->num_cem : p.max_cem;
+  }
+  p.bp = (max_bands + 15) / 16 * 16;
+  for (int i = 0; i < n; ++i) {
+    const hsi_frame& f = *frames[i];
+    p.frames[i] = f;
+    const int64_t P = static_cast<int64_t>(f.height) * f.width;
+    const int rc = encode_cube_map_sw128(&p.maps[i], f.cube, HSI_F16, P, f.bands, f.plane_stride, 64, p.bp);
+    if (rc != HSI_OK) return rc;
+  }
+  const int most = p.max_sam > p.max_cem ? p.max_sam : p.max_cem;
+  const int passes = static_cast<int>(div_up(most, kFiltersPerPass));
+  for (int pass = 0; pass < passes; ++pass) {
+    p.pass = pass;
+    const int rc = dispatch_h(round_h(pass_count_host(p.max_sam, pass)), round_h(pass_count_host(p.max_cem, pass)),
+                              p, s);
+    if (rc != HSI_OK) return rc;
+  }
+  return HSI_OK;
+}
+
+// FP32-FMA scorer over up to 64 validated frames of one element type.
+int score_fma_group(const hsi_frame* const* frames, int n, int* status, cudaStream_t s) {
+  static ScoreParams p;  // 8 KB: kept off the stack; the launch copies it
+  p = ScoreParams{};
+  p.table = nullptr;
+  p.num_frames = n;
+  p.status = status;
+  int max_bands = 0, max_sam = 0, max_cem = 0;
+  for (int i = 0; i < n; ++i) {
+    p.inline_frames[i] = *frames[i];
+    max_bands = frames[i]->bands > max_bands ? frames[i]->bands : max_bands;
+    max_sam = frames[i]->num_sam > max_sam ? frames[i]->num_sam : max_sam;
+    max_cem = frames[i]->num_cem > max_cem ? frames[i]->num_cem : max_cem;
+  }
+  return run_passes(p, frames[0]->dtype, max_bands, max_sam, max_cem, 0, s);
+}
+
+std::mutex g_host_frames_mutex;  // the group launchers keep their parameter blocks in statics
+
+// Frames whose descriptors are on the host: FP16 cubes of at most 128 bands
+// go to the tensor-core scorer, the rest to the FP32-FMA scorer, 64 frames
+// per launch.
+int score_host_frames(const hsi_frame* frames, int n, int* status, cudaStream_t s) {
+  if (!frames || n <= 0) return HSI_E_INVALID;
+  for (int i = 0; i < n; ++i) {
+    const int rc = validate_frame(frames[i]);
+    if (rc != HSI_OK) return rc;
+  }
+  std::lock_guard<std::mutex> lock(g_host_frames_mutex);
+  const hsi_frame* group[3][kMaxInline];  // tensor-core fp16, FMA fp32, FMA fp16
+  int count[3] = {0, 0, 0};
+  auto flush = [&](int g) -> int {
+    if (count[g] == 0) return HSI_OK;
+    const int rc = g == 0 ? score_h_group(group[0], count[0], status, s) : score_fma_group(group[g], count[g], status, s);
+    count[g] = 0;
+    return rc;
+  };
+  for (int i = 0; i < n; ++i) {
+    const int g = tensor_core_frame(frames[i]) ? 0 : (frames[i].dtype == HSI_F32 ? 1 : 2);
+    group[g][count[g]++] = &frames[i];
+    if (count[g] == kMaxInline) {
+      const int rc = flush(g);
+      if (rc != HSI_OK) return rc;
+    }
+  }
+  for (int g = 0; g < 3; ++g) {
+    const int rc = flush(g);
+    if (rc != HSI_OK) return rc;
+  }
+  return HSI_OK;
+}
+
 }  // namespace
 }  // namespace hsi_b200
 
 using namespace hsi_b200;
 
+extern "C" HSI_API int hsi_score_frames_batch(const hsi_frame* frames, int num_frames, int* d_status,
+                                              hsi_stream_t stream) {
+  return score_host_frames(frames, num_frames, d_status, reinterpret_cast<cudaStream_t>(stream));
+}
+
 extern "C" HSI_API int hsi_score_frames(const hsi_frame* frames, int num_frames, hsi_stream_t stream) {
   if (!frames || num_frames <= 0 || num_frames > HSI_MAX_INLINE_FRAMES) return HSI_E_INVALID;
-  ScoreParams p{};
-  p.table = nullptr;
-  p.num_frames = num_frames;
-  p.status = nullptr;
-  int max_bands = 0, max_sam = 0, max_cem = 0;
-  const int dtype = frames[0].dtype;
-  for (int i = 0; i < num_frames; ++i) {
-    const int rc = validate_frame(frames[i]);
-    if (rc != HSI_OK) return rc;
-    if (frames[i].dtype != dtype) return HSI_E_INVALID;
-    p.inline_frames[i] = frames[i];
-    max_bands = frames[i].bands > max_bands ? frames[i].bands : max_bands;
-    max_sam = frames[i].num_sam > max_sam ? frames[i].num_sam : max_sam;
-    max_cem = frames[i].num_cem > max_cem ? frames[i].num_cem : max_cem;
-  }
-  return run_passes(p, dtype, max_bands, max_sam, max_cem, 0, reinterpret_cast<cudaStream_t>(stream));
+  // one element type per call, as before
+  for (int i = 1; i < num_frames; ++i)
+    if (frames[i].dtype != frames[0].dtype) return HSI_E_INVALID;
+  return score_host_frames(frames, num_frames, nullptr, reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" HSI_API int hsi_score_frames_device_grid(const hsi_frame* d_frames, int num_frames, int dtype,

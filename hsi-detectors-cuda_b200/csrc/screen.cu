@@ -398,21 +398,6 @@ __global__ void __launch_bounds__(256) pack_kernel(const float* __restrict__ par
   if (threadIdx.x == 0) ops->b3 = v.b3[0];
 }
 
-// Shared-memory descriptor of an MN-major operand in the 128-byte swizzle:
-// 64 elements of 16 bits (128 B) along M per atom, atoms `mn_stride` bytes
-// apart; 8-row groups along K 1024 B apart.
-__device__ __forceinline__ uint64_t smem_desc_mn_sw128(const void* base, uint32_t mn_stride) {
-  const uint64_t start = (smem_addr(base) & 0x3FFFFu) >> 4;
-  const uint64_t lbo = (mn_stride >> 4) & 0x3FFFu;
-  const uint64_t sbo = 1024 >> 4;
-  return start | (lbo << 16) | (sbo << 32) | (1ull << 46) | (2ull << 61);
-}
-
-// F16 x F16 -> F32 with A MN-major (pixels contiguous), B K-major.
-__host__ __device__ constexpr uint32_t idesc_f16_amn(int m, int n) {
-  return (1u << 4) | (1u << 15) | (static_cast<uint32_t>(n >> 3) << 17) | (static_cast<uint32_t>(m >> 4) << 24);
-}
-
 struct ScreenArgs {
   int64_t pixels;
   int bands_padded;

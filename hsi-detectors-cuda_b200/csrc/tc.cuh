@@ -41,6 +41,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&r)[32]) {
       : "r"(addr));
 }
 
+// 32 lanes x 8 consecutive 32-bit columns.
+__device__ __forceinline__ void tmem_ld8(uint32_t addr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(addr));
+}
+
 // 32 lanes x 16 consecutive 32-bit columns.
 __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
   asm volatile(
@@ -73,6 +80,21 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(const void* tile) {
   const uint64_t lbo = 1;                 // unused for swizzled K-major tiles
   const uint64_t sbo = 1024 >> 4;         // byte distance between 8-row atoms
   return start | (lbo << 16) | (sbo << 32) | (1ull << 46) /* version */ | (2ull << 61) /* SWIZZLE_128B */;
+}
+
+// Shared-memory descriptor of an MN-major operand in the 128-byte swizzle:
+// 64 elements of 16 bits (128 B) along M per atom, atoms `mn_stride` bytes
+// apart; 8-row groups along K 1024 B apart.
+__device__ __forceinline__ uint64_t smem_desc_mn_sw128(const void* base, uint32_t mn_stride) {
+  const uint64_t start = (smem_addr(base) & 0x3FFFFu) >> 4;
+  const uint64_t lbo = (mn_stride >> 4) & 0x3FFFu;
+  const uint64_t sbo = 1024 >> 4;
+  return start | (lbo << 16) | (sbo << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// F16 x F16 -> F32 with A MN-major (pixels contiguous), B K-major.
+__host__ __device__ constexpr uint32_t idesc_f16_amn(int m, int n) {
+  return (1u << 4) | (1u << 15) | (static_cast<uint32_t>(n >> 3) << 17) | (static_cast<uint32_t>(m >> 4) << 24);
 }
 
 // Instruction descriptor: BF16 x BF16 -> FP32, both operands K-major.

@@ -129,6 +129,8 @@ def _optional_symbols(L):
         "hsi_scene_moments": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
         "hsi_scene_moments_simt": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
         "hsi_scene_moments_tc": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, C.c_size_t, vp], i32),
+        "hsi_score_frames_device_grid": ([vp, i32, i32, i32, i32, i32, vp, i32, vp], i32),
+        "hsi_score_frames_batch": ([vp, i32, vp, vp], i32),
         "hsi_scene_moments_batch_workspace_bytes": ([C.POINTER(MomentsJob), i32], C.c_size_t),
         "hsi_scene_moments_batch": ([C.POINTER(MomentsJob), i32, vp, C.c_size_t, vp], i32),
         "hsi_statistics_elements": ([i32, i32], C.c_size_t),
@@ -268,6 +270,15 @@ def score_frames(frames, stream=None) -> None:
     n = len(frames)
     arr = (Frame * n)(*frames)
     check(lib().hsi_score_frames(arr, n, _stream(stream)), "hsi_score_frames")
+
+
+def score_frames_batch(frames, status=None, stream=None) -> None:
+    """Any number of frames with host descriptors (Frame structs): FP16 cubes of at
+    most 128 bands on the tensor cores, the rest on the FP32-FMA scorer."""
+    n = len(frames)
+    arr = (Frame * n)(*frames)
+    check(lib().hsi_score_frames_batch(C.cast(arr, C.c_void_p), n, _ptr(status), _stream(stream)),
+          "hsi_score_frames_batch")
 
 
 def frame_table(frames, device="cuda"):

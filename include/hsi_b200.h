@@ -162,6 +162,16 @@ typedef struct hsi_frame {
 #define HSI_MAX_INLINE_FRAMES 4
 HSI_API int hsi_score_frames(const hsi_frame* frames, int num_frames, hsi_stream_t stream);
 
+/* Any number of frames whose descriptors are on the HOST, element types
+ * mixed, up to 64 per launch.  FP16 cubes of at most 128 bands are scored on
+ * the tensor cores: the cube is fed by TMA straight into tcgen05.mma.kind::f16
+ * (fp16 values are exact operands), each filter is scaled by a power of two
+ * and split into an fp16 head and remainder (22 significant bits), FP32
+ * accumulation.  Other frames take the FP32-FMA scorer.  Semantics, outputs
+ * and `d_status` (nullable) as hsi_score_frames_device; hsi_score_frames
+ * takes the same route for its frames. */
+HSI_API int hsi_score_frames_batch(const hsi_frame* frames, int num_frames, int* d_status, hsi_stream_t stream);
+
 /* Same for a descriptor table already in DEVICE memory: up to 256 frames of
  * uneven sizes, band counts and libraries in one persistent launch per pass.
  * Every frame must have element type `dtype`, at most `max_bands` bands,

@@ -218,6 +218,80 @@ def test_sam_and_cem_banks_of_uneven_sizes(hsi, orc, max_sam, max_cem):
             _check_cem(orc, host, cem, r)
 
 
+@pytest.mark.parametrize("B", [16, 113, 128])
+@pytest.mark.parametrize("T", [(8, 8), (3, 0), (0, 5), (16, 16), (20, 9)])
+def test_fp16_tensor_core_and_fma_scorers_match_the_oracle(hsi, orc, B, T):
+    """FP16 cubes of at most 128 bands with host descriptors take the
+    tensor-core scorer; descriptors in device memory take the FP32-FMA scorer.
+    Both must meet the same tolerances against the FP64 oracle, including
+    passes of more than 16 filters of a kind (20 SAM targets: two passes that
+    carry the best), CEM weights of small magnitude (the per-filter power-of-two
+    scale), and a last tile shorter than 128 pixels."""
+    ns, nc = T
+    H, W = 37, 101
+    sc = hsi.scene(B, n_targets=max(ns, nc, 1), target_frac=0.03, frame_seed=500 + B + ns, library_seed=61 + nc)
+    cube, _ = hsi.generate(sc, H, W, dtype=1)
+    host = _download(cube, B, H * W)
+    lib = hsi.scene_targets(sc)
+    rng = np.random.default_rng(B + 7 * nc)
+    cem = (rng.standard_normal((nc, B)) * 1e-3).astype(np.float32) if nc else None
+    P = H * W
+    for tensor_cores in (True, False):
+        kw, out = {}, {}
+        if ns:
+            kw["sam_targets"] = torch.from_numpy(np.ascontiguousarray(lib[:ns])).cuda()
+            kw["sam_norms"] = torch.from_numpy(hsi.target_norms(lib[:ns])).cuda()
+            out["sam_best"] = torch.full((P,), -7.0, device="cuda")
+            out["sam_best_target"] = torch.full((P,), -7, dtype=torch.int32, device="cuda")
+            out["sam_maps"] = torch.full((ns, P), -7.0, device="cuda")
+        if nc:
+            kw["cem_weights"] = torch.from_numpy(cem).cuda()
+            out["cem_best"] = torch.full((P,), -7.0, device="cuda")
+            out["cem_best_target"] = torch.full((P,), -7, dtype=torch.int32, device="cuda")
+            out["cem_maps"] = torch.full((nc, P), -7.0, device="cuda")
+        frame = hsi.make_frame(cube, H, W, B, 1, map_stride=P, **kw, **out)
+        status = torch.zeros(1, dtype=torch.int32, device="cuda")
+        if tensor_cores:
+            hsi.score_frames_batch([frame], status=status)
+        else:
+            hsi.score_frames_device(hsi.frame_table([frame]), 1, max_bands=B, max_sam=ns, max_cem=nc, dtype=1,
+                                    status=status)
+        torch.cuda.synchronize()
+        assert int(status.item()) == 0
+        r = {k: v.cpu().numpy() for k, v in out.items()}
+        if ns:
+            _check_sam(orc, host, lib[:ns], r["sam_best"], r["sam_best_target"], r["sam_maps"])
+        if nc:
+            _check_cem(orc, host, cem, r)
+
+
+def test_batch_entry_mixes_element_types(hsi, orc):
+    """One hsi_score_frames_batch call with FP32 and FP16 frames of several band
+    counts (FP16 above 128 bands falls back to the FP32-FMA scorer)."""
+    specs = [(113, 0), (113, 1), (224, 1), (16, 1), (60, 0)]
+    frames, keep = [], []
+    for i, (B, dt) in enumerate(specs):
+        H, W = 50, 70 + 3 * i
+        sc = hsi.scene(B, n_targets=4, target_frac=0.02, frame_seed=900 + i, library_seed=70 + i)
+        cube, _ = hsi.generate(sc, H, W, dtype=dt)
+        lib = hsi.scene_targets(sc)
+        P = H * W
+        best = torch.full((P,), -7.0, device="cuda")
+        bt = torch.full((P,), -7, dtype=torch.int32, device="cuda")
+        maps = torch.full((4, P), -7.0, device="cuda")
+        # descriptors hold raw pointers: every tensor they name stays referenced until the scorer is done
+        d_lib = torch.from_numpy(lib).cuda()
+        d_norms = torch.from_numpy(hsi.target_norms(lib)).cuda()
+        frames.append(hsi.make_frame(cube, H, W, B, dt, sam_targets=d_lib, sam_norms=d_norms, sam_maps=maps,
+                                     sam_best=best, sam_best_target=bt, map_stride=P))
+        keep.append((cube, lib, best, bt, maps, H, W, B, d_lib, d_norms))
+    hsi.score_frames_batch(frames)
+    torch.cuda.synchronize()
+    for cube, lib, best, bt, maps, H, W, B, _, _ in keep:
+        host = _download(cube, B, H * W)
+        _check_sam(orc, host, lib, best.cpu().numpy(), bt.cpu().numpy(), maps.cpu().numpy())
+
+
 def test_batched_frames_inline_and_device_table(hsi, orc):
     shapes = [(30, 41, 113), (64, 32, 16), (17, 19, 224)]
     frames, keep = [], []
