@@ -685,7 +685,7 @@ __global__ void __launch_bounds__(score_groups<KS, KC>() * kGroupThreads + 32, f
 constexpr int kHTile = 128;
 constexpr int kHStages = 6;
 constexpr int kHMaxBands = 128;
-constexpr int kHAcc = 4;  // TMEM accumulators (and norm buffers) in flight
+constexpr int kHAcc = 8;  // TMEM accumulators (and norm buffers) in flight
 constexpr int kHThreads = 22 * 32;
 
 struct HSmem {
@@ -730,7 +730,7 @@ template <int KS, int KC>
 __global__ void __launch_bounds__(kHThreads, 1) score_h_kernel(const __grid_constant__ HParams prm) {
   constexpr int N = (KS + KC + 15) / 16 * 16;
   constexpr int N2 = 2 * N;
-  constexpr uint32_t kCols = kHAcc * N2;  // 128 or 256 TMEM columns
+  constexpr uint32_t kCols = kHAcc * N2;  // 256 or 512 TMEM columns
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int bp = prm.bp;
@@ -881,16 +881,9 @@ __global__ void __launch_bounds__(kHThreads, 1) score_h_kernel(const __grid_cons
       const int f = fcur = next_frame(prefix, nframes, tile, fcur);
       const hsi_frame& F = prm.frames[f];
       if (f != cur) {
-        if (epoch > 0 && !mbar_wait(filt_free, (epoch - 1) & 1u)) {
-          ok = false;
-          break;
-        }
-        if (!mbar_wait(&sc_empty[epoch & 1u], ((epoch >> 1) & 1u) ^ 1u)) {
-          ok = false;
-          break;
-        }
-        // filter n: heads in row n, remainders in row N + n; bp / 8 threads per filter... here
-        // 128 / N threads per filter, each over every (128 / N)-th band
+        // filter n: heads in row n, remainders in row N + n; 128 / N threads per
+        // filter, each over every (128 / N)-th band.  The new frame's values are
+        // fetched before waiting for the MMAs on the old bank to complete.
         const int tpf = 128 / N, n = rt / tpf, j0 = rt % tpf;
         const int n_s = pass_count(F.num_sam, prm.pass), n_c = pass_count(F.num_cem, prm.pass);
         const int t0 = prm.pass * kFiltersPerPass;
@@ -900,18 +893,36 @@ __global__ void __launch_bounds__(kHThreads, 1) score_h_kernel(const __grid_cons
         } else if (n - KS < KC && n - KS < n_c) {
           src = F.cem_weights + static_cast<int64_t>(t0 + n - KS) * F.bands;
         }
+        float v[N];  // bands j0 + i tpf, i < N, cover 0..127
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          const int b = j0 + i * tpf;
+          v[i] = (src && b < F.bands) ? src[b] : 0.0f;
+        }
+        const float nr = (n < KS && n < n_s) ? F.sam_norms[t0 + n] : 0.0f;
         float mx = 0.0f;
-        for (int b = j0; b < F.bands; b += tpf)
-          if (src) mx = fmaxf(mx, fabsf(src[b]));
+#pragma unroll
+        for (int i = 0; i < N; ++i) mx = fmaxf(mx, fabsf(v[i]));
         for (int o = tpf / 2; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         int e2 = 0;
         if (mx > 0.0f) frexpf(mx, &e2);  // mx in [2^(e2-1), 2^e2)
         const float up = ldexpf(1.0f, -e2);
+        if (epoch > 0 && !mbar_wait(filt_free, (epoch - 1) & 1u)) {
+          ok = false;
+          break;
+        }
+        if (!mbar_wait(&sc_empty[epoch & 1u], ((epoch >> 1) & 1u) ^ 1u)) {
+          ok = false;
+          break;
+        }
         unsigned char* filt = smem + L.filt_off;
-        for (int b = j0; b < bp; b += tpf) {
-          const float v = (src && b < F.bands) ? src[b] * up : 0.0f;
-          const __half h = __float2half_rn(v);
-          const __half l = __float2half_rn(v - __half2float(h));
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          const int b = j0 + i * tpf;
+          if (b >= bp) break;
+          const float w = v[i] * up;
+          const __half h = __float2half_rn(w);
+          const __half l = __float2half_rn(w - __half2float(h));
           const int k2 = (b & 63) * 2;
           const uint32_t row_h = static_cast<uint32_t>(n), row_l = static_cast<uint32_t>(N + n);
           const uint32_t base = static_cast<uint32_t>((b >> 6) * N2 * 128);
@@ -922,10 +933,7 @@ __global__ void __launch_bounds__(kHThreads, 1) score_h_kernel(const __grid_cons
         }
         // multiplier of column pair n: x.f = (x.fh + x.fl) 2^e2, and SAM folds in 1 / |r_t|
         float mult = ldexpf(1.0f, e2);
-        if (n < KS) {
-          const float nr = n < n_s ? F.sam_norms[t0 + n] : 0.0f;
-          mult = nr > 0.0f ? mult / nr : 0.0f;
-        }
+        if (n < KS) mult = nr > 0.0f ? mult / nr : 0.0f;
         float* sc = reinterpret_cast<float*>(smem + L.scale_off) + (epoch & 1u) * 32;
         if (j0 == 0) sc[n] = mult;
         fence_proxy_async_smem();
