@@ -1286,7 +1286,11 @@ int dispatch_h(int ks, int kc, const HParams& p, cudaStream_t s) {
   }
 }
 
-bool tensor_core_frame(const hsi_frame& f) { return f.dtype == HSI_F16 && f.bands <= kHMaxBands; }
+// TMA pixel coordinates are 32-bit: larger frames stay on the FMA scorer.
+bool tensor_core_frame(const hsi_frame& f) {
+  const int64_t P = static_cast<int64_t>(f.height) * f.width;
+  return f.dtype == HSI_F16 && f.bands <= kHMaxBands && P <= (int64_t(1) << 31) - 256;
+}
 
 // Tensor-core scorer over up to 64 validated FP16 frames: a 2-D tensor map
 // (128-byte swizzle, boxes of 64 pixels x all bands) per cube, one launch per

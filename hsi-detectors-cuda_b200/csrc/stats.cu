@@ -21,7 +21,7 @@
 //   INT8 too, and four exact INT32 accumulators
 //     A0 = sum D D^T,  A1 = sum D L1^T,  A2 = sum (L1 L1^T + D L2^T),
 //     A3 = sum L1 L2^T
-//   (tcgen05.mma kind::i8, five MMAs per K-step).  F = 2^30 A0 + 2^24 A1 +
+//   (tcgen05.mma kind::i8, three MMAs per K-step, two of them N = 256).  F = 2^30 A0 + 2^24 A1 +
 //   2^16 A2 + 2^9 A3 and S = (F + F^T)/2 is sum q q^T except the weight-1
 //   products L2 L2^T: their diagonal is added back exactly (the converters
 //   count sum L2^2 per band), and of their off-diagonal sums the mean part
@@ -314,6 +314,10 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
   } else if (warp == kWarpMma) {
     if (lane == 0) {
       const uint32_t idesc = idesc_s8_s32(kRows, kRows);
+      // D, L1 and L2 are consecutive 128-row tiles, so [D; L1] and [L1; L2] are
+      // 256-row B operands: one N = 256 MMA reads its A tile once for two
+      // accumulators (A0 | A1 and A2 | A3 are adjacent in TMEM).
+      const uint32_t idesc_wide = idesc_s8_s32(kRows, 2 * kRows);
       uint32_t i = 0, chunk = 0;  // K-blocks and chunks issued so far
       bool ok = true;
       for (int f = walk.first(); ok && walk.in_range(f); ++f) {
@@ -346,11 +350,9 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
           for (int k = 0; k < kKB / 32; ++k) {
             const uint64_t adv = static_cast<uint64_t>(k * 2);  // 32 bytes of K, in 16-byte units
             const uint32_t acc = (j > 0 || k > 0) ? 1u : 0u;
-            umma_i8(tmem + 0, dd + adv, dd + adv, idesc, acc);    // A0 = D D^T
-            umma_i8(tmem + 128, dd + adv, d1 + adv, idesc, acc);  // A1 = D L1^T
-            umma_i8(tmem + 256, d1 + adv, d1 + adv, idesc, acc);  // A2 = L1 L1^T
-            umma_i8(tmem + 256, dd + adv, d2 + adv, idesc, 1u);   //    + D L2^T
-            umma_i8(tmem + 384, d1 + adv, d2 + adv, idesc, acc);  // A3 = L1 L2^T
+            umma_i8(tmem + 0, dd + adv, dd + adv, idesc_wide, acc);    // A0 | A1 = D [D; L1]^T
+            umma_i8(tmem + 256, d1 + adv, d1 + adv, idesc_wide, acc);  // A2 | A3 = L1 [L1; L2]^T
+            umma_i8(tmem + 256, dd + adv, d2 + adv, idesc, 1u);        // A2 += D L2^T
           }
           umma_commit(&op_empty[so]);
           if (j == kChunkKB - 1 || kb == hi - 1) {
