@@ -451,17 +451,33 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
 #pragma unroll
           for (int t2 = 0; t2 < kSlots; ++t2) {
             const int b = band0 + 32 * t2;
+            const uint32_t o = (o0 + 4096u * t2) ^ (half ? 64u : 0u);
+            if (b > B) {
+              // rows past the ones row: zero limbs (the buffer may hold another frame's rows)
+              *reinterpret_cast<uint32_t*>(op + o) = 0u;
+              *reinterpret_cast<uint32_t*>(op + kLimbBytes + o) = 0u;
+              *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + o) = 0u;
+              continue;
+            }
             uint32_t y[4] = {kZeroBits, kZeroBits, kZeroBits, kZeroBits};
             if (b < B) {
               const float4 x = load4f<T>(in + b * kBoxPx + sub_off + lp);
               const float xv[4] = {x.x, x.y, x.z, x.w};
-              // fully unrolled with a predicate: a loop bounded by nvalid would
-              // index y[] dynamically and move it to local memory
+              if (nvalid == 4) {
 #pragma unroll
-              for (int e = 0; e < 4; ++e) {
-                if (e < nvalid) {
+                for (int e = 0; e < 4; ++e) {
                   y[e] = __float_as_uint(fmaf(xv[e], sc[t2], off[t2]));
                   chk |= y[e] ^ kExpBits;
+                }
+              } else {
+                // fully unrolled with a predicate: a loop bounded by nvalid would
+                // index y[] dynamically and move it to local memory
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                  if (e < nvalid) {
+                    y[e] = __float_as_uint(fmaf(xv[e], sc[t2], off[t2]));
+                    chk |= y[e] ^ kExpBits;
+                  }
                 }
               }
             } else if (b == B) {
@@ -478,7 +494,6 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
             l2sq[t2] = static_cast<unsigned int>(
                 __dp4a(static_cast<int>(l2), static_cast<int>(l2), static_cast<int>(l2sq[t2])));
             l2s[t2] = __dp4a(static_cast<int>(l2), 0x01010101, l2s[t2]);
-            const uint32_t o = (o0 + 4096u * t2) ^ (half ? 64u : 0u);
             *reinterpret_cast<uint32_t*>(op + o) = dl;
             *reinterpret_cast<uint32_t*>(op + kLimbBytes + o) = l1;
             *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + o) = l2;
