@@ -32,6 +32,8 @@
 // TMEM: S0 columns [0,128), S1 [128,256), S2 [256,384), S3 [384,512).
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 #include "tc.cuh"
 
 namespace hsi_b200 {
@@ -121,8 +123,9 @@ __device__ __forceinline__ uint32_t sw128_byte(int row, int k) {
   return static_cast<uint32_t>((row >> 3) * 1024 + (row & 7) * 128 + ((((k >> 4) ^ (row & 7))) << 4) + (k & 15));
 }
 
-__device__ __forceinline__ float to_f(float v) { return v; }
-__device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
+// Two consecutive elements (8- or 4-byte aligned) as floats.
+__device__ __forceinline__ float2 load2f(const float* p) { return *reinterpret_cast<const float2*>(p); }
+__device__ __forceinline__ float2 load2f(const __half* p) { return __half22float2(*reinterpret_cast<const __half2*>(p)); }
 
 
 // ---- prep: the augmented matrix in fixed point, FP64 ------------------------
@@ -317,7 +320,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp < kWarpEpi0) {
     // ---------------- converters ----------------
-    // warp c owns bands [16c, 16c+16); lane l owns box pixels l and l + 32.
+    // warp c owns bands [16c, 16c+16); lane l owns box pixels 2l and 2l + 1 (one
+    // 64- or 32-bit load per band for both).
     const int c = warp - kWarpConv0;
     constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
     const int wbias = __float_as_int(kMagic) - 0x8080;
@@ -339,17 +343,27 @@ __global__ void __launch_bounds__(kThreads, 1)
       float* r = red + (j & 1) * kConvWarps * kBoxPx;
       float d[2][16];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int pl = lane + 32 * h;
-        const bool valid = tile * kTilePx + half * kBoxPx + pl < P;
-        float m = 0.0f;
+      for (int jj = 0; jj < 16; ++jj) {
+        const float2 x = load2f(in + (c * 16 + jj) * kBoxPx + 2 * lane);
+        d[0][jj] = x.x - mu[jj];
+        d[1][jj] = x.y - mu[jj];
+      }
+      // pixels past the frame (last tile only) convert as zeros
+      const int64_t px0 = tile * kTilePx + half * kBoxPx + 2 * lane;
+      if (px0 + 1 >= P) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj) d[h][jj] = px0 + h < P ? d[h][jj] : 0.0f;
+      }
+      {
+        float m0 = 0.0f, m1 = 0.0f;
 #pragma unroll
         for (int jj = 0; jj < 16; ++jj) {
-          const float x = to_f(in[(c * 16 + jj) * kBoxPx + pl]);
-          d[h][jj] = valid ? x - mu[jj] : 0.0f;
-          m = fmaxf(m, fabsf(d[h][jj]));
+          m0 = fmaxf(m0, fabsf(d[0][jj]));
+          m1 = fmaxf(m1, fabsf(d[1][jj]));
         }
-        r[c * kBoxPx + pl] = m;
+        *reinterpret_cast<float2*>(r + c * kBoxPx + 2 * lane) = make_float2(m0, m1);
       }
       // the input box is consumed (values are in registers); maxima published
       __syncwarp();
@@ -363,12 +377,17 @@ __global__ void __launch_bounds__(kThreads, 1)
         break;
       }
       unsigned char* a = smem + L.a_off + static_cast<size_t>(so) * 3 * kLimbBytes;
+      float2 mx = make_float2(0.0f, 0.0f);
+#pragma unroll
+      for (int cc = 0; cc < kConvWarps; ++cc) {
+        const float2 v = *reinterpret_cast<const float2*>(r + cc * kBoxPx + 2 * lane);
+        mx.x = fmaxf(mx.x, v.x);
+        mx.y = fmaxf(mx.y, v.y);
+      }
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int pl = lane + 32 * h;
-        float m = 0.0f;
-#pragma unroll
-        for (int cc = 0; cc < kConvWarps; ++cc) m = fmaxf(m, r[cc * kBoxPx + pl]);
+        const int pl = 2 * lane + h;
+        const float m = h ? mx.y : mx.x;
         // 2^t with m 2^t in [2^21, 2^22): |q| <= 2^22, exact through the FMA rounding
         int t = 0;
         if (m > 0.0f) t = min(max(21 - (static_cast<int>((__float_as_uint(m) >> 23) & 255u) - 127), -100), 100);
@@ -435,29 +454,38 @@ __global__ void __launch_bounds__(kThreads, 1)
         tmem_ld16(trow + 256 + n0, s2);
         tmem_ld16(trow + 384 + n0, s3);
         tmem_wait_ld();
+        // all_bands: every row of the block is a whitened band (the common case: no
+        // per-row test); otherwise rows past B are ACE numerators, past `rows` unused
+        auto block = [&](auto all_bands) {
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-          // four rows' gains and offsets per float4 broadcast (n0 is a multiple of 16)
-          const float4 gv = *reinterpret_cast<const float4*>(gain + n0 + 4 * v);
-          const float4 ov = *reinterpret_cast<const float4*>(offset + n0 + 4 * v);
-          const float g[4] = {gv.x, gv.y, gv.z, gv.w}, o[4] = {ov.x, ov.y, ov.z, ov.w};
+          for (int v = 0; v < 4; ++v) {
+            // four rows' gains and offsets per float4 broadcast (n0 is a multiple of 16)
+            const float4 gv = *reinterpret_cast<const float4*>(gain + n0 + 4 * v);
+            const float4 ov = *reinterpret_cast<const float4*>(offset + n0 + 4 * v);
+            const float g[4] = {gv.x, gv.y, gv.z, gv.w}, o[4] = {ov.x, ov.y, ov.z, ov.w};
 #pragma unroll
-          for (int jj = 0; jj < 4; ++jj) {
-            const int j = 4 * v + jj;
-            const int nn = n0 + j;
-            // u = S0 2^24 + S1 2^16 + S2 2^8 + S3 as (S0 256 + S1) 2^16 + (S2 256 + S3):
-            // |S0| <= 2^20, |S1| < 2^21.6, |S2| < 2^22.3, |S3| <= 2^22 (128 bands of
-            // |L0| <= 64, other limbs <= 128 in magnitude), so both halves are exact int32
-            const int hi = static_cast<int>(s0[j]) * 256 + static_cast<int>(s1[j]);
-            const int lo = static_cast<int>(s2[j]) * 256 + static_cast<int>(s3[j]);
-            const float u = fmaf(__int2float_rn(hi), 65536.0f, __int2float_rn(lo));
-            const float z = fmaf(u * tau, g[jj], o[jj]);
-            if (nn < B) {
-              zz = fmaf(z, z, zz);
-            } else if (nn < rows) {
-              zbuf[(nn - B) * kTilePx + px] = z;
+            for (int jj = 0; jj < 4; ++jj) {
+              const int j = 4 * v + jj;
+              const int nn = n0 + j;
+              // u = S0 2^24 + S1 2^16 + S2 2^8 + S3 as (S0 256 + S1) 2^16 + (S2 256 + S3):
+              // |S0| <= 2^20, |S1| < 2^21.6, |S2| < 2^22.3, |S3| <= 2^22 (128 bands of
+              // |L0| <= 64, other limbs <= 128 in magnitude), so both halves are exact int32
+              const int hi = static_cast<int>(s0[j]) * 256 + static_cast<int>(s1[j]);
+              const int lo = static_cast<int>(s2[j]) * 256 + static_cast<int>(s3[j]);
+              const float u = fmaf(__int2float_rn(hi), 65536.0f, __int2float_rn(lo));
+              const float z = fmaf(u * tau, g[jj], o[jj]);
+              if (decltype(all_bands)::value || nn < B) {
+                zz = fmaf(z, z, zz);
+              } else if (nn < rows) {
+                zbuf[(nn - B) * kTilePx + px] = z;
+              }
             }
           }
+        };
+        if (n0 + 16 <= B) {
+          block(std::true_type{});
+        } else {
+          block(std::false_type{});
         }
       }
       tc_fence_before();
