@@ -29,7 +29,13 @@
 //   warp 1      TMEM allocator + single-thread MMA issuer
 //   warps 2-9   converters: per-pixel scale, limb tiles in the UMMA layout
 //   warps 10-17 epilogue: TMEM -> z -> RX, ACE maps, best target
-// TMEM: S0 columns [0,128), S1 [128,256), S2 [256,384), S3 [384,512).
+// Two MMA rounds per tile, one per half of the output rows, each into its own
+// half of TMEM: round h (rows [64h, 64h + 64)) writes S0 to columns
+// [256h, 256h + 64), S1 the next 64, S2 and S3 after them.  The epilogue warps
+// of row half h drain round h while the MMAs of the other round run, so the
+// tensor cores no longer wait for the whole tile's epilogue.  In shared memory
+// the whitener limbs are laid out by row half, [M0 | M1 | M2] of rows 0-63 and
+// then of rows 64-127 (8 KB each), so [M0; M1] of a half is one 128-row operand.
 #include <cuda_fp16.h>
 
 #include <type_traits>
@@ -96,7 +102,7 @@ __host__ __device__ inline Smem smem_layout() {
   s.zb_off = off;                   // [16][128] ACE numerators
   off += kMaxTargetsPerPass * kTilePx * sizeof(float);
   s.bar_off = off;
-  off += (2 * 4 + 2 * kOpStages + 4 + 2 + 8) * sizeof(uint64_t);
+  off += (2 * 4 + 2 * kOpStages + 6 + 2 + 8) * sizeof(uint64_t);
   s.slot_off = off;
   off += 16;
   s.total = off + 1024;
@@ -203,9 +209,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* in_empty = bars + 4;
   uint64_t* op_full = bars + 8;
   uint64_t* op_empty = op_full + kOpStages;
-  uint64_t* acc_full = op_empty + kOpStages;
-  uint64_t* acc_empty = acc_full + 1;
-  uint64_t* w_full = acc_empty + 1;
+  uint64_t* acc_full = op_empty + kOpStages;  // [2]: one per row half
+  uint64_t* acc_empty = acc_full + 2;         // [2]
+  uint64_t* w_full = acc_empty + 2;
   uint64_t* mma_done = w_full + 1;
   uint64_t* red_bar = mma_done + 1;   // [2]: converters' per-box maxima written
   uint64_t* pair_bar = red_bar + 2;   // [4][2]: the two epilogue warps of a TMEM lane quarter
@@ -235,8 +241,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&op_full[s], kConvWarps);
       mbar_init(&op_empty[s], 1 + kEpiWarps);  // MMA done with the limbs + epilogue done with the scales
     }
-    mbar_init(acc_full, 1);
-    mbar_init(acc_empty, kEpiWarps);
+    for (int h = 0; h < 2; ++h) {
+      mbar_init(&acc_full[h], 1);
+      mbar_init(&acc_empty[h], kEpiWarps / 2);  // the epilogue warps of that row half
+    }
     mbar_init(w_full, 1);
     mbar_init(mma_done, 1);
     for (int b = 0; b < 2; ++b) mbar_init(&red_bar[b], kConvWarps);
@@ -254,9 +262,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == kWarpTma) {
     if (lane == 0) {
       prefetch_tensormap(&cube_map);
-      // the whitener limbs, once
+      // the whitener limbs, once, by row half: limb l of rows [64h, 64h + 64) at (3h + l) x 8 KB
       mbar_arrive_expect_tx(w_full, 3 * kLimbBytes);
-      for (int l = 0; l < 3; ++l) bulk_g2s(smem + L.w_off + l * kLimbBytes, args.ops->limbs[l], kLimbBytes, w_full);
+      for (int h = 0; h < 2; ++h)
+        for (int l = 0; l < 3; ++l)
+          bulk_g2s(smem + L.w_off + (3 * h + l) * (kLimbBytes / 2), args.ops->limbs[l] + h * (kLimbBytes / 2),
+                   kLimbBytes / 2, w_full);
       uint32_t pending = 0, parity = 0;
       for (int i = 0; i < 2 * n; ++i) {
         const int s = i % kIn;
@@ -279,39 +290,50 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == kWarpMma) {
     if (lane == 0) {
-      const uint32_t id256 = idesc_s8_s32(kTilePx, 2 * kRows);
-      const uint32_t id128 = idesc_s8_s32(kTilePx, kRows);
+      const uint32_t id128 = idesc_s8_s32(kTilePx, kRows);      // [M0; M1] of a row half
+      const uint32_t id64 = idesc_s8_s32(kTilePx, kRows / 2);   // M2 of a row half
       bool issued = false;
       if (n > 0 && !mbar_wait(w_full, 0)) {
         record_error(args.status, HSI_E_TIMEOUT);
         *abort_flag = 1;
       }
-      const uint64_t bw01 = smem_desc_sw128(smem + L.w_off);                   // [M0; M1], 256 rows
-      const uint64_t bw2 = smem_desc_sw128(smem + L.w_off + 2 * kLimbBytes);   // M2
-      for (int i = 0; i < n && !*abort_flag; ++i) {
+      bool ok = true;
+      for (int i = 0; i < n && ok && !*abort_flag; ++i) {
         const int so = i % kOpStages;
-        if (!mbar_wait(acc_empty, (i & 1u) ^ 1u) || !mbar_wait(&op_full[so], (i / kOpStages) & 1u)) {
+        if (!mbar_wait(&op_full[so], (i / kOpStages) & 1u)) {
           record_error(args.status, HSI_E_TIMEOUT);
           *abort_flag = 1;
           break;
         }
-        tc_fence_after();
         unsigned char* a = smem + L.a_off + static_cast<size_t>(so) * 3 * kLimbBytes;
         const uint64_t a0 = smem_desc_sw128(a), a1 = smem_desc_sw128(a + kLimbBytes);
         const uint64_t a2 = smem_desc_sw128(a + 2 * kLimbBytes);
+        for (int h = 0; h < 2; ++h) {
+          if (!mbar_wait(&acc_empty[h], (i & 1u) ^ 1u)) {
+            record_error(args.status, HSI_E_TIMEOUT);
+            *abort_flag = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d = tmem + 256u * h;  // S0 | S1 | S2 | S3 of this row half, 64 columns each
+          const uint64_t bw01 = smem_desc_sw128(smem + L.w_off + 3 * h * (kLimbBytes / 2));      // [M0; M1]
+          const uint64_t bw2 = smem_desc_sw128(smem + L.w_off + (3 * h + 2) * (kLimbBytes / 2));  // M2
 #pragma unroll
-        for (int k = 0; k < kK / 32; ++k) {
-          const uint64_t adv = static_cast<uint64_t>(k * 2);  // 32 bytes of K in 16-byte units
-          const uint32_t acc = k > 0 ? 1u : 0u;
-          umma_i8(tmem + 256, a2 + adv, bw01 + adv, id256, acc);  // S2 += L2 M0, S3 += L2 M1
-          umma_i8(tmem + 0, a0 + adv, bw01 + adv, id256, acc);    // S0 += L0 M0, S1 += L0 M1
-          umma_i8(tmem + 128, a1 + adv, bw01 + adv, id256, 1u);   // S1 += L1 M0, S2 += L1 M1
-          umma_i8(tmem + 256, a0 + adv, bw2 + adv, id128, 1u);    // S2 += L0 M2
-          umma_i8(tmem + 384, a1 + adv, bw2 + adv, id128, 1u);    // S3 += L1 M2
+          for (int k = 0; k < kK / 32; ++k) {
+            const uint64_t adv = static_cast<uint64_t>(k * 2);  // 32 bytes of K in 16-byte units
+            const uint32_t acc = k > 0 ? 1u : 0u;
+            umma_i8(d + 128, a2 + adv, bw01 + adv, id128, acc);  // S2 += L2 M0, S3 += L2 M1
+            umma_i8(d + 0, a0 + adv, bw01 + adv, id128, acc);    // S0 += L0 M0, S1 += L0 M1
+            umma_i8(d + 64, a1 + adv, bw01 + adv, id128, 1u);    // S1 += L1 M0, S2 += L1 M1
+            umma_i8(d + 128, a0 + adv, bw2 + adv, id64, 1u);     // S2 += L0 M2
+            umma_i8(d + 192, a1 + adv, bw2 + adv, id64, 1u);     // S3 += L1 M2
+          }
+          umma_commit(&acc_full[h]);
+          issued = true;
         }
+        if (!ok) break;
         umma_commit(&op_empty[so]);
-        umma_commit(acc_full);
-        issued = true;
       }
       if (issued) {
         umma_commit(mma_done);
@@ -427,7 +449,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int B = args.bands, rows = args.rows, nt = args.ntarg;
     for (int i = 0; i < n; ++i) {
       const int so = i % kOpStages;
-      if (!mbar_wait(acc_full, i & 1u)) {
+      if (!mbar_wait(&acc_full[hf], i & 1u)) {
         record_error(args.status, HSI_E_TIMEOUT);
         *abort_flag = 1;
         break;
@@ -449,10 +471,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int n0 = hf * 64 + cb * 16;
         if (n0 >= rows) break;  // warp-uniform
         uint32_t s0[16], s1[16], s2[16], s3[16];
-        tmem_ld16(trow + 0 + n0, s0);
-        tmem_ld16(trow + 128 + n0, s1);
-        tmem_ld16(trow + 256 + n0, s2);
-        tmem_ld16(trow + 384 + n0, s3);
+        const uint32_t col = 256u * hf + 16u * cb;  // rows n0.. of this half's S0; S1, S2, S3 64 columns apart
+        tmem_ld16(trow + col, s0);
+        tmem_ld16(trow + col + 64, s1);
+        tmem_ld16(trow + col + 128, s2);
+        tmem_ld16(trow + col + 192, s3);
         tmem_wait_ld();
         // all_bands: every row of the block is a whitened band (the common case: no
         // per-row test); otherwise rows past B are ACE numerators, past `rows` unused
@@ -490,7 +513,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(acc_empty);
+      if (lane == 0) mbar_arrive(&acc_empty[hf]);
       zzp[hf * kTilePx + px] = zz;
       __syncwarp();
       if (lane == 0) mbar_arrive(&pair_bar[q * 2 + 0]);
