@@ -74,3 +74,36 @@ def test_device_spectra_match_oracle_spectra():
     np.testing.assert_array_equal(sp[:6], em)
     np.testing.assert_array_equal(sp[6:11], tg)
     np.testing.assert_array_equal(sp[11], an)
+
+
+def _fake_frame(hsi, **over):
+    """A descriptor that passes host validation, with aligned device addresses
+    that are never dereferenced (every case below fails validation first)."""
+    base = 1 << 40
+    f = hsi.Frame()
+    f.cube, f.plane_stride, f.height, f.width, f.bands, f.dtype = base, 4096, 64, 64, 113, hsi.F16
+    f.sam_targets, f.sam_norms, f.num_sam = base + 0x100000, base + 0x200000, 8
+    f.num_cem, f.cem_weights = 8, base + 0x300000
+    f.sam_best, f.sam_best_target, f.map_stride = base + 0x400000, base + 0x500000, 4096
+    for k, v in over.items():
+        setattr(f, k, v)
+    return f
+
+
+@pytest.mark.parametrize("bad", [
+    dict(bands=0), dict(bands=257), dict(dtype=2), dict(height=0), dict(plane_stride=4000),
+    dict(plane_stride=4100), dict(cube=(1 << 40) + 8), dict(num_sam=0, num_cem=0), dict(sam_targets=None),
+    dict(sam_norms=None), dict(cem_weights=None), dict(sam_maps=1 << 41, map_stride=100),
+    dict(num_sam=20, sam_best=None),
+])
+def test_batch_scoring_validates_every_descriptor_before_any_launch(bad):
+    """hsi_score_frames_batch checks every host descriptor before it groups or
+    launches anything: one bad frame among good ones fails the whole call with
+    HSI_E_INVALID, so these run without a GPU."""
+    import hsi_b200 as hsi
+    L = hsi.lib()
+    frames = [_fake_frame(hsi), _fake_frame(hsi, dtype=hsi.F32), _fake_frame(hsi, **bad)]
+    arr = (hsi.Frame * len(frames))(*frames)
+    assert L.hsi_score_frames_batch(C.cast(arr, C.c_void_p), len(frames), None, None) == hsi.E_INVALID
+    assert L.hsi_score_frames_batch(None, 1, None, None) == hsi.E_INVALID
+    assert L.hsi_score_frames_batch(C.cast(arr, C.c_void_p), 0, None, None) == hsi.E_INVALID
