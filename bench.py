@@ -207,18 +207,50 @@ def workload_config(workload, frames, reference=False):
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+    """SM clocks and throttle reasons sampled while the timed region runs: NVML
+    read-only queries from a thread every 5 ms (a region of tens of ms still gets
+    a dozen samples), else nvidia-smi every 200 ms.  Nothing is set."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
     def __init__(self, uuid):
         self.uuid = uuid
         self.proc = None
         self.file = None
+        self.thread = None
+        self.samples = []  # (sm MHz, reason bits)
+        self.max_mhz = None
+
+    def _nvml_start(self):
+        import threading
+        import pynvml
+        pynvml.nvmlInit()
+        h = (pynvml.nvmlDeviceGetHandleByUUID(self.uuid.encode()) if self.uuid
+             else pynvml.nvmlDeviceGetHandleByIndex(0))
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        self.stop = threading.Event()
+
+        def run():
+            while not self.stop.is_set():
+                try:
+                    self.samples.append((float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)),
+                                         int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                except Exception:
+                    pass
+                self.stop.wait(0.005)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def __enter__(self):
+        try:
+            self._nvml_start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
@@ -230,6 +262,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -238,6 +273,12 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        if self.thread is not None:
+            if not self.samples:
+                return None
+            reasons = {n for n, bit in self.REASONS.items() if any(r & bit for _, r in self.samples)}
+            return {"sm_mhz": float(np.median([m for m, _ in self.samples])), "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(reasons), "samples": len(self.samples), "source": "nvml, 5 ms"}
         if self.file is None:
             return None
         try:
@@ -259,7 +300,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 class Workload:
