@@ -973,6 +973,123 @@ __global__ void __launch_bounds__(256) simt_finalize_kernel(const double* __rest
 }
 
 // ---------------------------------------------------------------------------
+// Frames of 128..254 bands.  Two contiguous band views of at most 127 bands
+// take the exact tensor-core moments as one launch sequence.  Only the cross
+// block between them runs on the CUDA cores, each band referenced to its mean
+// from the views.  An FP64 assembly gives the frame's raw moments.  The
+// CUDA-core work is the h x (B - h) block instead of the whole lower triangle.
+// ---------------------------------------------------------------------------
+// Mean of band b of a view's raw moments (nb bands), rounded to FP32: the
+// reference the cross sums subtract.
+__device__ __forceinline__ double view_ref(const double* m, int nb, int b) {
+  return static_cast<double>(static_cast<float>(m[b] / m[nb + nb * nb]));
+}
+
+// Block (ti, tj) of the cross sums over a pixel slice: rows a = view-1 bands
+// [64 ti, 64 ti + 64) (frame bands h + a), columns c = view-0 bands [64 tj, ...).
+// FP32 products of mean-referenced values, summed over each 32-pixel step, then
+// FP64, as the CUDA-core moments.
+template <typename T>
+__global__ void __launch_bounds__(256, 3) stats_cross_kernel(const T* __restrict__ cube, int64_t pixels, int64_t stride,
+                                                         int h, int n1, const double* __restrict__ m0,
+                                                         const double* __restrict__ m1, double* __restrict__ partials,
+                                                         int slices, int ct, int nrp, int ncp) {
+  const int ti = blockIdx.y / ct, tj = blockIdx.y % ct;
+  __shared__ float si[kSimtPx][kSimtTile + 4];
+  __shared__ float sj[kSimtPx][kSimtTile + 4];
+  __shared__ float ri[kSimtTile], rj[kSimtTile];
+  for (int k = threadIdx.x; k < kSimtTile; k += blockDim.x) {
+    const int a = ti * kSimtTile + k, c = tj * kSimtTile + k;
+    ri[k] = a < n1 ? static_cast<float>(view_ref(m1, n1, a)) : 0.0f;
+    rj[k] = c < h ? static_cast<float>(view_ref(m0, h, c)) : 0.0f;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  float acc[4][4];
+  double dacc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      acc[r][c] = 0.0f;
+      dacc[r][c] = 0.0;
+    }
+  const int64_t per = div_up<int64_t>(pixels, slices);
+  const int64_t p0 = per * blockIdx.x, p1 = min(pixels, p0 + per);
+  for (int64_t base = p0; base < p1; base += kSimtPx) {
+    for (int e = threadIdx.x; e < kSimtPx * kSimtTile; e += blockDim.x) {
+      const int px = e % kSimtPx, rb = e / kSimtPx;
+      const int64_t p = base + px;
+      const int a = ti * kSimtTile + rb, c = tj * kSimtTile + rb;
+      float vi = 0.0f, vj = 0.0f;
+      if (p < p1) {
+        if (a < n1) vi = static_cast<float>(cube[static_cast<int64_t>(h + a) * stride + p]) - ri[rb];
+        if (c < h) vj = static_cast<float>(cube[static_cast<int64_t>(c) * stride + p]) - rj[rb];
+      }
+      si[px][rb] = vi;
+      sj[px][rb] = vj;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int px = 0; px < kSimtPx; ++px) {
+      const float4 x = *reinterpret_cast<const float4*>(&si[px][ty * 4]);
+      const float4 y = *reinterpret_cast<const float4*>(&sj[px][tx * 4]);
+      const float xv[4] = {x.x, x.y, x.z, x.w}, yv[4] = {y.x, y.y, y.z, y.w};
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(xv[r], yv[c], acc[r][c]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        dacc[r][c] += acc[r][c];
+        acc[r][c] = 0.0f;
+      }
+  }
+  // partial layout: [slice][column c][row a] over the padded ncp x nrp block
+  double* out = partials + static_cast<size_t>(blockIdx.x) * nrp * ncp;
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      out[static_cast<size_t>(tj * kSimtTile + tx * 4 + c) * nrp + ti * kSimtTile + ty * 4 + r] = dacc[r][c];
+}
+
+// Raw moments [sum (B) | outer (B x B) | N] of the frame from the views' raw
+// moments (m0: bands [0, h), m1: bands [h, B)) and the cross sums.  With the
+// references r used by the cross kernel,
+//   sum_p x_a x_c = C_ac + r_c S_a + r_a S_c - N r_a r_c.
+__global__ void __launch_bounds__(256) split_assemble_kernel(const double* __restrict__ m0,
+                                                            const double* __restrict__ m1,
+                                                            const double* __restrict__ partials, int slices, int h,
+                                                            int n1, int nrp, int ncp, double* __restrict__ moments) {
+  const int B = h + n1;
+  const double N = m0[h + h * h];
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e < B) moments[e] = e < h ? m0[e] : m1[e - h];
+  if (e == 0) moments[B + static_cast<int64_t>(B) * B] = N;
+  if (e >= static_cast<int64_t>(B) * B) return;
+  const int i = static_cast<int>(e / B), j = static_cast<int>(e % B);
+  double v;
+  if (i < h && j < h) {
+    v = m0[h + i * h + j];
+  } else if (i >= h && j >= h) {
+    v = m1[n1 + (i - h) * n1 + (j - h)];
+  } else {
+    const int a = i >= h ? i - h : j - h;  // view-1 band
+    const int c = i >= h ? j : i;          // view-0 band
+    double C = 0.0;
+    for (int sl = 0; sl < slices; ++sl) C += partials[static_cast<size_t>(sl) * nrp * ncp + static_cast<size_t>(c) * nrp + a];
+    const double ra = view_ref(m1, n1, a), rc = view_ref(m0, h, c);
+    v = C + rc * m1[a] + ra * m0[c] - N * ra * rc;
+  }
+  moments[B + e] = v;
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 
@@ -1003,6 +1120,37 @@ size_t simt_ws_bytes(int bands) {
   const int n = ((bands + 1 + kSimtTile - 1) / kSimtTile) * kSimtTile;
   return align256(sizeof(StatsState)) + align256(static_cast<size_t>(kSimtSlices) * n * n * sizeof(double)) +
          align256(static_cast<size_t>(n) * n * sizeof(double));
+}
+
+// Split path (128..254 bands): view 0 holds bands [0, h), view 1 bands [h, B).
+constexpr int kSplitMaxBands = 2 * kMaxTensorBands;
+
+struct SplitDims {
+  int h, n1;     // bands of the two views
+  int rt, ct;    // 64-band tiles of the cross block (rows: view 1, columns: view 0)
+  int nrp, ncp;  // padded rows and columns
+};
+
+SplitDims split_dims(int bands) {
+  SplitDims d;
+  d.h = (bands + 1) / 2;
+  d.n1 = bands - d.h;
+  d.rt = (d.n1 + kSimtTile - 1) / kSimtTile;
+  d.ct = (d.h + kSimtTile - 1) / kSimtTile;
+  d.nrp = d.rt * kSimtTile;
+  d.ncp = d.ct * kSimtTile;
+  return d;
+}
+
+size_t view_moments_bytes(int bands) {
+  return align256((static_cast<size_t>(bands) + static_cast<size_t>(bands) * bands + 1) * sizeof(double));
+}
+
+// The two views' tensor-core workspace, their moments, the cross partials.
+size_t split_ws_bytes(int bands) {
+  const SplitDims d = split_dims(bands);
+  return tensor_ws_bytes(2) + view_moments_bytes(d.h) + view_moments_bytes(d.n1) +
+         align256(static_cast<size_t>(kSimtSlices) * d.nrp * d.ncp * sizeof(double));
 }
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -1139,6 +1287,34 @@ int launch_simt_stats(const hsi_moments_job& j, void* workspace, cudaStream_t s)
   return static_cast<int>(cudaGetLastError());
 }
 
+template <typename T>
+int launch_split_stats(const hsi_moments_job& j, void* workspace, cudaStream_t s) {
+  const SplitDims d = split_dims(j.bands);
+  const int64_t P = static_cast<int64_t>(j.height) * j.width;
+  unsigned char* w = static_cast<unsigned char*>(workspace) + tensor_ws_bytes(2);
+  double* m0 = reinterpret_cast<double*>(w);
+  double* m1 = reinterpret_cast<double*>(w + view_moments_bytes(d.h));
+  double* partials = reinterpret_cast<double*>(w + view_moments_bytes(d.h) + view_moments_bytes(d.n1));
+  hsi_moments_job v0 = j, v1 = j;
+  v0.bands = d.h;
+  v0.moments = m0;
+  v1.bands = d.n1;
+  v1.moments = m1;
+  // plane h: 16-byte aligned, as the plane stride is a multiple of 8 elements
+  v1.cube = static_cast<const unsigned char*>(j.cube) + static_cast<size_t>(d.h) * j.plane_stride * sizeof(T);
+  v1.reference = j.reference ? j.reference + d.h : nullptr;
+  const hsi_moments_job* views[2] = {&v0, &v1};
+  const int rc = launch_tensor_group<T>(views, 2, workspace, s, nullptr);
+  if (rc != HSI_OK) return rc;
+  stats_cross_kernel<T><<<dim3(kSimtSlices, d.rt * d.ct), 256, 0, s>>>(
+      static_cast<const T*>(j.cube), P, j.plane_stride, d.h, d.n1, m0, m1, partials, kSimtSlices, d.ct, d.nrp,
+      d.ncp);
+  const int64_t BB = static_cast<int64_t>(j.bands) * j.bands;
+  split_assemble_kernel<<<static_cast<unsigned>((BB + 255) / 256), 256, 0, s>>>(m0, m1, partials, kSimtSlices, d.h,
+                                                                              d.n1, d.nrp, d.ncp, j.moments);
+  return static_cast<int>(cudaGetLastError());
+}
+
 int check_job(const hsi_moments_job& j) {
   if (!j.cube || !j.moments || j.height <= 0 || j.width <= 0 || j.bands <= 0 || j.bands > HSI_MAX_BANDS)
     return HSI_E_INVALID;
@@ -1156,9 +1332,15 @@ bool tensor_capable(const hsi_moments_job& j) {
 
 // Default routing: small frames (where the integer path's one approximation,
 // the off-diagonal sums of the lowest limbs' products, is largest relative to
-// the sums, and the work is cheap) and bands >= 128 take the FP32 CUDA-core path.
+// the sums, and the work is cheap) take the FP32 CUDA-core path; larger frames
+// of at most 127 bands the tensor path, of 128..254 bands the split path.
 bool tensor_default(const hsi_moments_job& j) {
   return tensor_capable(j) && static_cast<int64_t>(j.height) * j.width >= kTensorMinPixels;
+}
+
+bool split_default(const hsi_moments_job& j) {
+  const int64_t P = static_cast<int64_t>(j.height) * j.width;
+  return j.bands > kMaxTensorBands && j.bands <= kSplitMaxBands && P >= kTensorMinPixels && P < kTensorMaxPixels;
 }
 
 enum class Route { kDefault, kSimt, kTensor };
@@ -1191,6 +1373,8 @@ int run_jobs(const hsi_moments_job* jobs, int n, void* ws, size_t ws_bytes, cuda
       const int d = j.dtype == HSI_F32 ? 0 : 1;
       group[d][count[d]++] = &j;
       if (count[d] == kMaxBatch) rc = flush(d);
+    } else if (route == Route::kDefault && split_default(j)) {
+      rc = j.dtype == HSI_F32 ? launch_split_stats<float>(j, ws, s) : launch_split_stats<__half>(j, ws, s);
     } else {
       rc = j.dtype == HSI_F32 ? launch_simt_stats<float>(j, ws, s) : launch_simt_stats<__half>(j, ws, s);
     }
@@ -1264,7 +1448,11 @@ extern "C" HSI_API size_t hsi_scene_moments_batch_workspace_bytes(const hsi_mome
   for (int i = 0; i < num_jobs; ++i) {
     if (jobs[i].bands <= 0 || jobs[i].bands > HSI_MAX_BANDS) return 0;
     // every job may be routed either way (the _tc and _simt entry points force one)
-    const size_t b = simt_ws_bytes(jobs[i].bands);
+    size_t b = simt_ws_bytes(jobs[i].bands);
+    if (jobs[i].bands > kMaxTensorBands && jobs[i].bands <= kSplitMaxBands) {
+      const size_t sb = split_ws_bytes(jobs[i].bands);
+      if (sb > b) b = sb;
+    }
     if (b > need) need = b;
     if (tensor_capable(jobs[i])) ++tensor;
   }
@@ -1284,7 +1472,9 @@ extern "C" HSI_API int hsi_scene_moments_batch(const hsi_moments_job* jobs, int 
 extern "C" HSI_API size_t hsi_stats_workspace_bytes(int height, int width, int bands) {
   if (height <= 0 || width <= 0 || bands <= 0 || bands > HSI_MAX_BANDS) return 0;
   const size_t a = tensor_ws_bytes(1), b = simt_ws_bytes(bands);
-  return a > b ? a : b;
+  const size_t c = bands > kMaxTensorBands && bands <= kSplitMaxBands ? split_ws_bytes(bands) : 0;
+  const size_t m = a > b ? a : b;
+  return m > c ? m : c;
 }
 
 extern "C" HSI_API int hsi_scene_moments(const void* d_cube, int height, int width, int bands, int dtype,

@@ -42,7 +42,7 @@ def _check_moments(hsi, orc, host, gm, B, P, cov_tol=5e-8, mean_tol=1e-7):
 
 
 @pytest.mark.parametrize("path", [None, "simt", "tc"])
-@pytest.mark.parametrize("B", [1, 3, 16, 113, 127, 128, 224])
+@pytest.mark.parametrize("B", [1, 3, 16, 113, 127, 128, 224, 254, 255])
 @pytest.mark.parametrize("shape", [(7, 13), (64, 64), (256, 300)])
 def test_moments_match_fp64(hsi, orc, path, B, shape):
     H, W = shape

@@ -136,3 +136,22 @@ def test_caller_reference_and_validation(hsi, orc):
     with pytest.raises(hsi.HsiError) as e:
         hsi.scene_moments_batch([hsi.moments_job(cube, H, W, B, out)], workspace=small)
     assert e.value.status == hsi.E_WORKSPACE
+
+
+def test_split_path_for_128_to_254_bands(hsi, orc):
+    """Frames of 128..254 bands and at least 32768 pixels take the split path:
+    two contiguous band views of at most 127 bands on the tensor cores (exact
+    integer sums) and the cross block between them on the CUDA cores.  Each
+    frame must meet the FP64 oracle at the tolerances above, be bit-identical
+    run to run, and equal its single-frame result inside a mixed batch."""
+    specs = [(224, 256, 300, 0), (113, 256, 256, 0), (224, 200, 200, 1), (254, 190, 190, 0), (128, 256, 256, 0)]
+    cubes = [_frame(hsi, B, H, W, dt, 0x5EED7400 + i) for i, (B, H, W, dt) in enumerate(specs)]
+    got = _run_batch(hsi, specs, cubes)
+    again = _run_batch(hsi, specs, cubes)
+    for i, ((B, H, W, dt), cube) in enumerate(zip(specs, cubes)):
+        single = hsi.scene_moments(cube, H, W, B, dtype=dt)
+        torch.cuda.synchronize()
+        assert torch.equal(got[i], single), i
+        assert torch.equal(got[i], again[i]), i
+        cov, mean = _cov_err(hsi, orc, cube, got[i], B, H * W)
+        assert cov < 5e-8 and mean < 1e-7, (i, cov, mean)
