@@ -988,21 +988,35 @@ __device__ __forceinline__ double view_ref(const double* m, int nb, int b) {
 // Block (ti, tj) of the cross sums over a pixel slice: rows a = view-1 bands
 // [64 ti, 64 ti + 64) (frame bands h + a), columns c = view-0 bands [64 tj, ...).
 // FP32 products of mean-referenced values, summed over each 32-pixel step, then
-// FP64, as the CUDA-core moments.
+// FP64, as the CUDA-core moments.  Staging is [row][pixel]: a warp loads 32
+// consecutive pixels of one band and stores them to 32 consecutive banks; the
+// math reads 4 pixels of a row per 128-bit load.  Thread (ty, tx) owns rows
+// ty + 16 r and columns tx + 16 c, so the 16 column rows a warp reads at once
+// are consecutive, and the row stride of 36 floats puts them on distinct bank
+// groups (two wavefronts).
+constexpr int kCrossStride = kSimtPx + 4;
+
 template <typename T>
 __global__ void __launch_bounds__(256, 3) stats_cross_kernel(const T* __restrict__ cube, int64_t pixels, int64_t stride,
-                                                         int h, int n1, const double* __restrict__ m0,
-                                                         const double* __restrict__ m1, double* __restrict__ partials,
-                                                         int slices, int ct, int nrp, int ncp) {
+                                                            int h, int n1, const double* __restrict__ m0,
+                                                            const double* __restrict__ m1, double* __restrict__ partials,
+                                                            int slices, int ct, int nrp, int ncp) {
   const int ti = blockIdx.y / ct, tj = blockIdx.y % ct;
-  __shared__ float si[kSimtPx][kSimtTile + 4];
-  __shared__ float sj[kSimtPx][kSimtTile + 4];
-  __shared__ float ri[kSimtTile], rj[kSimtTile];
-  for (int k = threadIdx.x; k < kSimtTile; k += blockDim.x) {
-    const int a = ti * kSimtTile + k, c = tj * kSimtTile + k;
-    ri[k] = a < n1 ? static_cast<float>(view_ref(m1, n1, a)) : 0.0f;
-    rj[k] = c < h ? static_cast<float>(view_ref(m0, h, c)) : 0.0f;
+  __shared__ __align__(16) float stage[2 * kSimtTile][kCrossStride];  // rows 0-63: a, 64-127: c
+  __shared__ float ref[2 * kSimtTile];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int k = threadIdx.x; k < 2 * kSimtTile; k += blockDim.x) {
+    const int a = ti * kSimtTile + k, c = tj * kSimtTile + (k - kSimtTile);
+    ref[k] = k < kSimtTile ? (a < n1 ? static_cast<float>(view_ref(m1, n1, a)) : 0.0f)
+                           : (c < h ? static_cast<float>(view_ref(m0, h, c)) : 0.0f);
   }
+  // staged rows of this thread: warp + 8 k, k < 16 (k < 8: a rows, then c rows);
+  // row a0 + 8 k of view 1 is frame band h + a0 + 8 k, row c0 + 8 k of view 0 band c0 + 8 k
+  constexpr int kRowsPerThread = 2 * kSimtTile / 8;
+  const int a0 = ti * kSimtTile + warp, c0 = tj * kSimtTile + warp;
+  const T* srcA = cube + static_cast<int64_t>(h + a0) * stride;
+  const T* srcC = cube + static_cast<int64_t>(c0) * stride;
+  const int64_t step8 = 8 * stride;
   __syncthreads();
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   float acc[4][4];
@@ -1016,29 +1030,38 @@ __global__ void __launch_bounds__(256, 3) stats_cross_kernel(const T* __restrict
     }
   const int64_t per = div_up<int64_t>(pixels, slices);
   const int64_t p0 = per * blockIdx.x, p1 = min(pixels, p0 + per);
-  for (int64_t base = p0; base < p1; base += kSimtPx) {
-    for (int e = threadIdx.x; e < kSimtPx * kSimtTile; e += blockDim.x) {
-      const int px = e % kSimtPx, rb = e / kSimtPx;
-      const int64_t p = base + px;
-      const int a = ti * kSimtTile + rb, c = tj * kSimtTile + rb;
-      float vi = 0.0f, vj = 0.0f;
-      if (p < p1) {
-        if (a < n1) vi = static_cast<float>(cube[static_cast<int64_t>(h + a) * stride + p]) - ri[rb];
-        if (c < h) vj = static_cast<float>(cube[static_cast<int64_t>(c) * stride + p]) - rj[rb];
-      }
-      si[px][rb] = vi;
-      sj[px][rb] = vj;
+  float nxt[kRowsPerThread];
+  auto fetch = [&](int64_t base) {
+    const int64_t p = base + lane;
+    const bool in = p < p1;
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread / 2; ++k) {
+      nxt[k] = (in && a0 + 8 * k < n1) ? static_cast<float>(srcA[k * step8 + p]) - ref[warp + 8 * k] : 0.0f;
+      nxt[k + kRowsPerThread / 2] =
+          (in && c0 + 8 * k < h) ? static_cast<float>(srcC[k * step8 + p]) - ref[kSimtTile + warp + 8 * k] : 0.0f;
     }
+  };
+  for (int64_t base = p0; base < p1; base += kSimtPx) {
+    fetch(base);
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread; ++k) stage[warp + 8 * k][lane] = nxt[k];
     __syncthreads();
-#pragma unroll 8
-    for (int px = 0; px < kSimtPx; ++px) {
-      const float4 x = *reinterpret_cast<const float4*>(&si[px][ty * 4]);
-      const float4 y = *reinterpret_cast<const float4*>(&sj[px][tx * 4]);
-      const float xv[4] = {x.x, x.y, x.z, x.w}, yv[4] = {y.x, y.y, y.z, y.w};
+#pragma unroll 2
+    for (int q = 0; q < kSimtPx; q += 4) {
+      float4 x[4], y[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) x[r] = *reinterpret_cast<const float4*>(&stage[ty + 16 * r][q]);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) y[c] = *reinterpret_cast<const float4*>(&stage[kSimtTile + tx + 16 * c][q]);
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(xv[r], yv[c], acc[r][c]);
+        for (int c = 0; c < 4; ++c) {
+          acc[r][c] = fmaf(x[r].x, y[c].x, acc[r][c]);
+          acc[r][c] = fmaf(x[r].y, y[c].y, acc[r][c]);
+          acc[r][c] = fmaf(x[r].z, y[c].z, acc[r][c]);
+          acc[r][c] = fmaf(x[r].w, y[c].w, acc[r][c]);
+        }
     }
     __syncthreads();
 #pragma unroll
@@ -1055,7 +1078,7 @@ __global__ void __launch_bounds__(256, 3) stats_cross_kernel(const T* __restrict
   for (int r = 0; r < 4; ++r)
 #pragma unroll
     for (int c = 0; c < 4; ++c)
-      out[static_cast<size_t>(tj * kSimtTile + tx * 4 + c) * nrp + ti * kSimtTile + ty * 4 + r] = dacc[r][c];
+      out[static_cast<size_t>(tj * kSimtTile + tx + 16 * c) * nrp + ti * kSimtTile + ty + 16 * r] = dacc[r][c];
 }
 
 // Raw moments [sum (B) | outer (B x B) | N] of the frame from the views' raw
