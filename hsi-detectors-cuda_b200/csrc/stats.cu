@@ -187,8 +187,15 @@ struct FrameStats {
   int bands;
   int cta_lo;              // first CTA whose K-block range meets this frame
   int nslots;
-  int pad;
+  int run0;                // bands in the first contiguous run of planes (== bands: one run)
+  int64_t run1_plane;      // first plane of the second run, counted from `cube`
 };
+
+// Plane of band b: a frame may be a view of two contiguous runs of a cube's
+// planes (bands [0, run0) at planes [0, run0), the rest from run1_plane on).
+__host__ __device__ __forceinline__ int64_t plane_of(const FrameStats& F, int b) {
+  return b < F.run0 ? b : F.run1_plane + (b - F.run0);
+}
 
 struct FrameTable {
   FrameStats f[kMaxBatch];
@@ -202,6 +209,7 @@ struct FrameTable {
 
 struct GemmParams {
   CUtensorMap maps[kMaxBatch];
+  CUtensorMap maps1[kMaxBatch];  // second run of a two-run frame
   FrameTable t;
   int conditional;  // 1: only frames whose re-run is armed
 };
@@ -301,8 +309,17 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
               break;
             }
             unsigned char* dst = smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>();
-            mbar_arrive_expect_tx(&in_full[s], in_tile_bytes<T>());
-            tma_load_2d(dst, map, static_cast<int>((kb - kbf) * kKB + half * kBoxPx), 0, &in_full[s]);
+            const int x = static_cast<int>((kb - kbf) * kKB + half * kBoxPx);
+            const FrameStats& Fp = t.f[f];
+            if (Fp.run0 < Fp.bands) {
+              // two runs: one box each, stacked in the tile's rows
+              mbar_arrive_expect_tx(&in_full[s], static_cast<uint32_t>(Fp.bands) * kBoxPx * sizeof(T));
+              tma_load_2d(dst, map, x, 0, &in_full[s]);
+              tma_load_2d(dst + static_cast<size_t>(Fp.run0) * kBoxPx * sizeof(T), &p.maps1[f], x, 0, &in_full[s]);
+            } else {
+              mbar_arrive_expect_tx(&in_full[s], in_tile_bytes<T>());
+              tma_load_2d(dst, map, x, 0, &in_full[s]);
+            }
             pending |= 1u << s;
             parity = (parity & ~(1u << s)) | (ph << s);
           }
@@ -657,7 +674,7 @@ __global__ void __launch_bounds__(256) shift_partial_kernel(const __grid_constan
   const FrameStats& F = t.f[blockIdx.z];
   const int b = blockIdx.x;
   if (b >= F.bands) return;
-  const T* plane = static_cast<const T*>(F.cube) + static_cast<int64_t>(b) * F.stride;
+  const T* plane = static_cast<const T*>(F.cube) + plane_of(F, b) * F.stride;
   const int64_t pixels = F.pixels;
   const int64_t runs = div_up<int64_t>(pixels, 64);
   const int64_t step = runs > 512 ? runs / 256 : 1;  // about 256 runs (16384 pixels) per band
@@ -745,7 +762,7 @@ __global__ void __launch_bounds__(256) range_kernel(const __grid_constant__ Fram
     const FrameStats& F = t.f[item / per_frame];
     const int b = (item % per_frame) / kShiftSplit, split = item % kShiftSplit;
     if (b >= F.bands || !(F.state->flags & 1)) continue;
-    const T* plane = static_cast<const T*>(F.cube) + static_cast<int64_t>(b) * F.stride;
+    const T* plane = static_cast<const T*>(F.cube) + plane_of(F, b) * F.stride;
     const int64_t per = div_up<int64_t>(F.pixels, kShiftSplit);
     const int64_t p0 = per * split, p1 = min(F.pixels, p0 + per);
     float lo = INFINITY, hi = -INFINITY;
@@ -1112,6 +1129,40 @@ __global__ void __launch_bounds__(256) split_assemble_kernel(const double* __res
   moments[B + e] = v;
 }
 
+// Frames of 128..252 bands with quarters Q0..Q3 of at most 63 bands (q: their
+// bounds).  Six exact tensor-core views: Q0 u Q1 and Q2 u Q3 (contiguous) for
+// the sums and the diagonal blocks, and Qi u Qj (two runs, i in {0, 1}, j in
+// {2, 3}) for the cross blocks.  Every entry of the frame's raw moments is an
+// entry of one view's raw moments.
+struct QuarterViews {
+  const double* m[6];  // raw moments [sum | outer | N] of each view
+  int nb[6];           // bands of each view
+  int q[5];            // quarter bounds
+};
+
+__global__ void __launch_bounds__(256) quarter_assemble_kernel(const __grid_constant__ QuarterViews v,
+                                                              double* __restrict__ moments) {
+  const int B = v.q[4], h = v.q[2];
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e < B) moments[e] = e < h ? v.m[0][e] : v.m[1][e - h];
+  if (e == 0) moments[B + static_cast<int64_t>(B) * B] = v.m[0][v.nb[0] + v.nb[0] * v.nb[0]];
+  if (e >= static_cast<int64_t>(B) * B) return;
+  const int i = static_cast<int>(e / B), k = static_cast<int>(e % B);
+  double val;
+  if (i < h && k < h) {
+    val = v.m[0][v.nb[0] + i * v.nb[0] + k];
+  } else if (i >= h && k >= h) {
+    val = v.m[1][v.nb[1] + (i - h) * v.nb[1] + (k - h)];
+  } else {
+    const int c = i < h ? i : k, a = i < h ? k : i;  // c in Q0 u Q1, a in Q2 u Q3
+    const int qc = c < v.q[1] ? 0 : 1, qa = a < v.q[3] ? 2 : 3;
+    const int w = 2 + 2 * qc + (qa - 2);
+    const int rc = c - v.q[qc], ra = (v.q[qc + 1] - v.q[qc]) + (a - v.q[qa]);
+    val = v.m[w][v.nb[w] + rc * v.nb[w] + ra];
+  }
+  moments[B + e] = val;
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -1169,11 +1220,50 @@ size_t view_moments_bytes(int bands) {
   return align256((static_cast<size_t>(bands) + static_cast<size_t>(bands) * bands + 1) * sizeof(double));
 }
 
-// The two views' tensor-core workspace, their moments, the cross partials.
+// Quarter views serve frames of up to 4 x 63 bands (two quarters per view).
+constexpr int kQuarterMaxBands = 4 * 63;
+
+struct QuarterDims {
+  int q[5];
+  int nb[6];
+  int64_t first[6];  // first plane of each view
+  int run0[6];
+  int64_t run1[6];   // second run's first plane, from the view's first plane
+};
+
+QuarterDims quarter_dims(int bands) {
+  QuarterDims d;
+  const int h = (bands + 1) / 2;
+  d.q[0] = 0;
+  d.q[1] = (h + 1) / 2;
+  d.q[2] = h;
+  d.q[3] = h + (bands - h + 1) / 2;
+  d.q[4] = bands;
+  d.nb[0] = h, d.first[0] = 0, d.run0[0] = h, d.run1[0] = 0;
+  d.nb[1] = bands - h, d.first[1] = h, d.run0[1] = bands - h, d.run1[1] = 0;
+  for (int i = 0; i < 2; ++i)
+    for (int j = 2; j < 4; ++j) {
+      const int w = 2 + 2 * i + (j - 2);
+      d.run0[w] = d.q[i + 1] - d.q[i];
+      d.nb[w] = d.run0[w] + (d.q[j + 1] - d.q[j]);
+      d.first[w] = d.q[i];
+      d.run1[w] = d.q[j] - d.q[i];
+    }
+  return d;
+}
+
+// The views' tensor-core workspace, their moments, and (two-view form) the cross partials.
 size_t split_ws_bytes(int bands) {
   const SplitDims d = split_dims(bands);
-  return tensor_ws_bytes(2) + view_moments_bytes(d.h) + view_moments_bytes(d.n1) +
-         align256(static_cast<size_t>(kSimtSlices) * d.nrp * d.ncp * sizeof(double));
+  size_t two = tensor_ws_bytes(2) + view_moments_bytes(d.h) + view_moments_bytes(d.n1) +
+               align256(static_cast<size_t>(kSimtSlices) * d.nrp * d.ncp * sizeof(double));
+  if (bands <= kQuarterMaxBands) {
+    const QuarterDims qd = quarter_dims(bands);
+    size_t four = tensor_ws_bytes(6);
+    for (int w = 0; w < 6; ++w) four += view_moments_bytes(qd.nb[w]);
+    if (four > two) two = four;
+  }
+  return two;
 }
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -1200,6 +1290,7 @@ FrameStats frame_of_job(const hsi_moments_job& j) {
   F.reference = j.reference;
   F.moments = j.moments;
   F.bands = j.bands;
+  F.run0 = j.bands;
   return F;
 }
 
@@ -1213,9 +1304,10 @@ void launch_shift(const FrameTable& t, cudaStream_t s) {
 // One launch sequence for m <= kMaxBatch frames of element type T, all on the
 // tensor path: shift + scale -> GEMM -> (conditional) range + rescale + GEMM
 // re-run -> exact reduction -> finalize.
+// run0 / run1_plane (nullable): frames that are two-run views of their cube.
 template <typename T>
 int launch_tensor_group(const hsi_moments_job* const* jobs, int m, void* workspace, cudaStream_t s,
-                        int* status) {
+                        int* status, const int* run0 = nullptr, const int64_t* run1_plane = nullptr) {
   static GemmParams p;  // large (13 KB): kept off the stack; calls are serialised by the caller's thread
   p = GemmParams{};
   FrameTable& t = p.t;
@@ -1227,8 +1319,23 @@ int launch_tensor_group(const hsi_moments_job* const* jobs, int m, void* workspa
     t.f[f].kb_begin = total;
     total += div_up<int64_t>(t.f[f].pixels, kKB);
     if (t.f[f].bands > t.max_bands) t.max_bands = t.f[f].bands;
-    const int rc = encode_cube_map(&p.maps[f], jobs[f]->cube, jobs[f]->dtype, t.f[f].pixels, t.f[f].bands,
-                                   t.f[f].stride, kBoxPx, kRows);
+    int rc;
+    if (run0 && run0[f] < t.f[f].bands) {
+      FrameStats& F = t.f[f];
+      F.run0 = run0[f];
+      F.run1_plane = run1_plane[f];
+      const int r1 = F.bands - F.run0;
+      const size_t esize = jobs[f]->dtype == HSI_F32 ? 4 : 2;
+      rc = encode_cube_map(&p.maps[f], jobs[f]->cube, jobs[f]->dtype, F.pixels, F.run0, F.stride, kBoxPx, F.run0);
+      if (rc == HSI_OK)
+        rc = encode_cube_map(&p.maps1[f],
+                             static_cast<const unsigned char*>(jobs[f]->cube) +
+                                 static_cast<size_t>(F.run1_plane) * F.stride * esize,
+                             jobs[f]->dtype, F.pixels, r1, F.stride, kBoxPx, r1);
+    } else {
+      rc = encode_cube_map(&p.maps[f], jobs[f]->cube, jobs[f]->dtype, t.f[f].pixels, t.f[f].bands,
+                           t.f[f].stride, kBoxPx, kRows);
+    }
     if (rc != HSI_OK) return rc;
   }
   t.total_kb = total;
@@ -1311,7 +1418,36 @@ int launch_simt_stats(const hsi_moments_job& j, void* workspace, cudaStream_t s)
 }
 
 template <typename T>
+int launch_quarter_stats(const hsi_moments_job& j, void* workspace, cudaStream_t s) {
+  const QuarterDims d = quarter_dims(j.bands);
+  unsigned char* w = static_cast<unsigned char*>(workspace) + tensor_ws_bytes(6);
+  hsi_moments_job v[6];
+  const hsi_moments_job* views[6];
+  QuarterViews qv;
+  for (int k = 0; k < 6; ++k) {
+    v[k] = j;
+    v[k].cube = static_cast<const unsigned char*>(j.cube) + static_cast<size_t>(d.first[k]) * j.plane_stride * sizeof(T);
+    v[k].bands = d.nb[k];
+    v[k].moments = reinterpret_cast<double*>(w);
+    v[k].reference = nullptr;
+    w += view_moments_bytes(d.nb[k]);
+    views[k] = &v[k];
+    qv.m[k] = v[k].moments;
+    qv.nb[k] = d.nb[k];
+  }
+  for (int k = 0; k < 5; ++k) qv.q[k] = d.q[k];
+  const int rc = launch_tensor_group<T>(views, 6, workspace, s, nullptr, d.run0, d.run1);
+  if (rc != HSI_OK) return rc;
+  const int64_t BB = static_cast<int64_t>(j.bands) * j.bands;
+  quarter_assemble_kernel<<<static_cast<unsigned>((BB + 255) / 256), 256, 0, s>>>(qv, j.moments);
+  return static_cast<int>(cudaGetLastError());
+}
+
+template <typename T>
 int launch_split_stats(const hsi_moments_job& j, void* workspace, cudaStream_t s) {
+  // all on the tensor cores when quarters fit (a caller's reference points
+  // apply to whole bands, so those frames keep the two-view form)
+  if (j.bands <= kQuarterMaxBands && !j.reference) return launch_quarter_stats<T>(j, workspace, s);
   const SplitDims d = split_dims(j.bands);
   const int64_t P = static_cast<int64_t>(j.height) * j.width;
   unsigned char* w = static_cast<unsigned char*>(workspace) + tensor_ws_bytes(2);
