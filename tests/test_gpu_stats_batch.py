@@ -155,3 +155,29 @@ def test_split_path_for_128_to_254_bands(hsi, orc):
         assert torch.equal(got[i], again[i]), i
         cov, mean = _cov_err(hsi, orc, cube, got[i], B, H * W)
         assert cov < 5e-8 and mean < 1e-7, (i, cov, mean)
+
+
+@pytest.mark.parametrize("B", [129, 201, 252, 253])
+def test_split_band_counts(hsi, orc, B):
+    """Odd and extreme band counts of the split paths: quarters of unequal size
+    (129, 201), the largest all-tensor-core frame (252 = 4 x 63) and the first
+    that keeps the CUDA-core cross block (253)."""
+    H, W = 200, 170
+    cube = _frame(hsi, B, H, W, 0, 0x5EED7500 + B)
+    got = _run_batch(hsi, [(B, H, W, 0)], [cube])[0]
+    single = hsi.scene_moments(cube, H, W, B)
+    torch.cuda.synchronize()
+    assert torch.equal(got, single)
+    cov, mean = _cov_err(hsi, orc, cube, got, B, H * W)
+    assert cov < 5e-8 and mean < 1e-7, (cov, mean)
+
+
+def test_split_path_with_caller_reference(hsi, orc):
+    """A caller's per-band reference points keep the two-view split form (the
+    references apply to whole bands); the result is as accurate."""
+    B, H, W = 224, 200, 200
+    cube = _frame(hsi, B, H, W, 0, 0x5EED7600)
+    ref = cube[:, :H * W].float().mean(1).contiguous()
+    got = _run_batch(hsi, [(B, H, W, 0)], [cube], refs=[ref])[0]
+    cov, mean = _cov_err(hsi, orc, cube, got, B, H * W)
+    assert cov < 5e-8 and mean < 1e-7, (cov, mean)
