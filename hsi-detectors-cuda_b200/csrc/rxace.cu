@@ -152,27 +152,40 @@ __global__ void __launch_bounds__(kThreads) rxace_simt_kernel(const T* __restric
     const int warp_rows_hi = r0 + (threadIdx.x >> 5) * 16 + 15;
     const bool warp_dense = warp_rows_hi >= B;
 
-    auto load = [&](int kc, int buf) {
+    // The cube elements of chunk kc + 1 are loaded into registers before chunk
+    // kc's FMAs and stored to the other buffer after them, so their latency
+    // overlaps the math.  W (a few hundred KB, resident in L2) is copied then.
+    constexpr int kPer = kKChunk * kPxTile / kThreads;  // 8 cube elements per thread
+    float yreg[kPer];
+    auto fetch = [&](int kc) {
       const int k0 = kc * kKChunk;
-      for (int e = threadIdx.x; e < kKChunk * kRowsTile; e += kThreads) {
-        const int r = e / kKChunk, k = e % kKChunk;
-        sm.w[buf][k][r] = op.waug[static_cast<size_t>(r0 + r) * op.kpad + k0 + k];
-      }
-      for (int e = threadIdx.x; e < kKChunk * kPxTile; e += kThreads) {
-        const int k = e / kPxTile, px = e % kPxTile;
-        const int b = k0 + k;
-        const int64_t p = p0 + px;
+#pragma unroll
+      for (int m = 0; m < kPer; ++m) {
+        const int e = threadIdx.x + kThreads * m;
+        const int b = k0 + e / kPxTile;
+        const int64_t p = p0 + e % kPxTile;
         float y = 0.0f;
         if (b < B && p < pixels)
           y = (to_f<T>(cube[static_cast<int64_t>(b) * stride + p]) - op.mean_hi[b]) - op.mean_lo[b];
-        sm.y[buf][k][px] = y;
+        yreg[m] = y;
       }
     };
-    load(0, 0);
+    auto commit = [&](int kc, int buf) {
+      const int k0 = kc * kKChunk;
+      for (int e = threadIdx.x; e < kKChunk * kRowsTile; e += kThreads)
+        sm.w[buf][e % kKChunk][e / kKChunk] = op.waug[static_cast<size_t>(r0 + e / kKChunk) * op.kpad + k0 + e % kKChunk];
+#pragma unroll
+      for (int m = 0; m < kPer; ++m) {
+        const int e = threadIdx.x + kThreads * m;
+        sm.y[buf][e / kPxTile][e % kPxTile] = yreg[m];
+      }
+    };
+    fetch(0);
+    commit(0, 0);
     __syncthreads();
     for (int kc = 0; kc < kchunks; ++kc) {
       const int buf = kc & 1;
-      if (kc + 1 < kchunks) load(kc + 1, buf ^ 1);
+      if (kc + 1 < kchunks) fetch(kc + 1);
       const bool skip = !warp_dense && kc * kKChunk > warp_rows_hi;
       if (!skip) {
 #pragma unroll
@@ -189,6 +202,8 @@ __global__ void __launch_bounds__(kThreads) rxace_simt_kernel(const T* __restric
             for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(wv[i], yv[j], acc[i][j]);
         }
       }
+      // buffer buf ^ 1 was last read in iteration kc - 1, before its closing barrier
+      if (kc + 1 < kchunks) commit(kc + 1, buf ^ 1);
       __syncthreads();
     }
     // fold: rows < B -> RX partials; rows B..B+T-1 -> ACE numerators
