@@ -124,7 +124,7 @@ struct SimtSmem {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) rxace_simt_kernel(const T* __restrict__ cube, int64_t pixels,
+__global__ void __launch_bounds__(kThreads, 2) rxace_simt_kernel(const T* __restrict__ cube, int64_t pixels,
                                                              int64_t stride, int B, int Tn, SimtOperands op,
                                                              ScoreOut out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -141,11 +141,11 @@ __global__ void __launch_bounds__(kThreads) rxace_simt_kernel(const T* __restric
 
   for (int rt = 0; rt < op.rows / kRowsTile; ++rt) {
     const int r0 = rt * kRowsTile;
-    float acc[8][8];
+    float2 acc[8][4];  // row i, pixels (2 j2, 2 j2 + 1) of this thread's 8: packed FMAs
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+      for (int j2 = 0; j2 < 4; ++j2) acc[i][j2] = make_float2(0.0f, 0.0f);
     // A warp owns rows r0 + 16w .. r0 + 16w + 15; W is zero above the
     // diagonal, so K-chunks past its last row contribute nothing unless the
     // warp also holds target rows (dense).
@@ -195,11 +195,14 @@ __global__ void __launch_bounds__(kThreads) rxace_simt_kernel(const T* __restric
           const float4 ya = *reinterpret_cast<const float4*>(&sm.y[buf][k][tx * 4]);
           const float4 yb = *reinterpret_cast<const float4*>(&sm.y[buf][k][64 + tx * 4]);
           const float wv[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
-          const float yv[8] = {ya.x, ya.y, ya.z, ya.w, yb.x, yb.y, yb.z, yb.w};
+          const float2 yv[4] = {make_float2(ya.x, ya.y), make_float2(ya.z, ya.w), make_float2(yb.x, yb.y),
+                                make_float2(yb.z, yb.w)};
 #pragma unroll
-          for (int i = 0; i < 8; ++i)
+          for (int i = 0; i < 8; ++i) {
+            const float2 wi = make_float2(wv[i], wv[i]);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(wv[i], yv[j], acc[i][j]);
+            for (int j2 = 0; j2 < 4; ++j2) acc[i][j2] = ffma2(wi, yv[j2], acc[i][j2]);
+          }
         }
       }
       // buffer buf ^ 1 was last read in iteration kc - 1, before its closing barrier
@@ -213,10 +216,11 @@ __global__ void __launch_bounds__(kThreads) rxace_simt_kernel(const T* __restric
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int px = j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4;
+        const float z = (j & 1) ? acc[i][j >> 1].y : acc[i][j >> 1].x;
         if (row < B) {
-          rx_part[j] = fmaf(acc[i][j], acc[i][j], rx_part[j]);
+          rx_part[j] = fmaf(z, z, rx_part[j]);
         } else if (row < B + Tn) {
-          sm.zu[row - B][px] = acc[i][j];
+          sm.zu[row - B][px] = z;
         }
       }
     }

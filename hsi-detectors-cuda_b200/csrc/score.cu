@@ -128,16 +128,6 @@ __host__ __device__ inline SmemLayout smem_layout(int groups, int max_bands, int
   return l;
 }
 
-// Packed FP32 FMA on sm_100: two lanes per instruction, d = a * b + c.
-__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
-  unsigned long long r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;"
-      : "=l"(r)
-      : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)),
-        "l"(*reinterpret_cast<unsigned long long*>(&c)));
-  return *reinterpret_cast<float2*>(&r);
-}
-
 // Accumulate one stage (nb bands) of this thread's 4 pixels against KG
 // filters.  Pixels are held as pairs (p0,p1), (p2,p3); the filter bank is
 // stored duplicated, (f,f), so a 128-bit shared load yields two filters ready
