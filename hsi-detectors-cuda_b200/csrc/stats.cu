@@ -154,7 +154,9 @@ __device__ __forceinline__ float4 load4f<__half>(const __half* p) {
   return make_float4(a.x, a.y, b.x, b.y);
 }
 
-constexpr int kShiftSplit = 16;  // blocks per band of the subsample and range passes
+constexpr int kShiftSplit = 16;  // slots per band of the subsample pass, blocks per band of the range pass
+constexpr int kShiftItems = 4;   // subsample slots per block
+constexpr int kShiftHeld = 4;    // loads per thread and slot issued ahead of the reduction
 
 // Per-frame state of the launch sequence.
 struct StatsState {
@@ -631,9 +633,12 @@ __global__ void shift_init_kernel(const __grid_constant__ FrameTable t) {
 
 // Block-wide sum / count (into this block's slot) and min / max (folded into
 // the frame's state with atomics).
-__device__ void fold_subsample(double sum, double cnt, float lo, float hi, StatsState* st, int b) {
+// Called once per slot by every thread of the block; the leading barrier
+// keeps a call's writes behind thread 0's reads of the one before.
+__device__ void fold_subsample(double sum, double cnt, float lo, float hi, StatsState* st, int b, int slot) {
   __shared__ double s_sum[8], s_cnt[8];
   __shared__ int s_lo[8], s_hi[8];
+  __syncthreads();
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -658,8 +663,8 @@ __device__ void fold_subsample(double sum, double cnt, float lo, float hi, Stats
       tl = min(tl, s_lo[w]);
       th = max(th, s_hi[w]);
     }
-    st->sub_sum[b][blockIdx.y] = ts;
-    st->sub_cnt[b][blockIdx.y] = tc;
+    st->sub_sum[b][slot] = ts;
+    st->sub_cnt[b][slot] = tc;
     if (tl <= th) {  // the block saw a value other than NaN
       atomicMin(&st->sub_lo[b], tl);
       atomicMax(&st->sub_hi[b], th);
@@ -667,8 +672,13 @@ __device__ void fold_subsample(double sum, double cnt, float lo, float hi, Stats
   }
 }
 
-// Subsample statistics, grid (bands, kShiftSplit, frames): runs of 64
-// pixels, about 256 of them per band on frames above 512 runs.
+// Subsample statistics, grid (bands, kShiftSplit / kShiftItems, frames):
+// runs of 64 pixels, about 256 of them per band on frames above 512 runs.
+// Each block takes kShiftItems consecutive slots and issues the first
+// kShiftHeld loads of every slot before reducing any, so that a block keeps
+// 16 loads per thread in flight; each slot's sums are still taken over the
+// same runs in the same order, so that the slots hold the same values at any
+// kShiftItems.
 template <typename T>
 __global__ void __launch_bounds__(256) shift_partial_kernel(const __grid_constant__ FrameTable t) {
   const FrameStats& F = t.f[blockIdx.z];
@@ -679,23 +689,59 @@ __global__ void __launch_bounds__(256) shift_partial_kernel(const __grid_constan
   const int64_t runs = div_up<int64_t>(pixels, 64);
   const int64_t step = runs > 512 ? runs / 256 : 1;  // about 256 runs (16384 pixels) per band
   const int64_t sampled = div_up<int64_t>(runs, step);
-  const int64_t r0 = sampled * blockIdx.y / kShiftSplit, r1 = sampled * (blockIdx.y + 1) / kShiftSplit;
-  double sum = 0.0, cnt = 0.0;
-  float lo = INFINITY, hi = -INFINITY;
-#pragma unroll 4
-  for (int64_t run = r0 + threadIdx.x / 64; run < r1; run += blockDim.x / 64) {
-    const int64_t px = run * step * 64 + (threadIdx.x & 63);
-    if (px < pixels) {
-      const float v = static_cast<float>(plane[px]);
-      if (t.center_mean) {
-        sum += static_cast<double>(v);
-        cnt += 1.0;
+  constexpr int kRowGroups = 256 / 64;  // runs a block covers per pass
+  const int row = threadIdx.x / 64, col = threadIdx.x & 63;
+  float held[kShiftItems][kShiftHeld];
+  unsigned valid = 0u;
+#pragma unroll
+  for (int i = 0; i < kShiftItems; ++i) {
+    const int slot = blockIdx.y * kShiftItems + i;
+    const int64_t r0 = sampled * slot / kShiftSplit, r1 = sampled * (slot + 1) / kShiftSplit;
+    const int64_t first = (r0 + row) * step * 64 + col;  // pixel of this thread's first run
+    const int count = static_cast<int>(r1 - r0);          // runs of the slot (at most 32)
+#pragma unroll
+    for (int k = 0; k < kShiftHeld; ++k) {
+      const int64_t px = first + static_cast<int64_t>(kRowGroups * k) * step * 64;
+      held[i][k] = 0.0f;
+      if (row + kRowGroups * k < count && px < pixels) {
+        held[i][k] = static_cast<float>(plane[px]);
+        valid |= 1u << (i * kShiftHeld + k);
       }
-      lo = fminf(lo, v);
-      hi = fmaxf(hi, v);
     }
   }
-  fold_subsample(sum, cnt, lo, hi, F.state, b);
+#pragma unroll
+  for (int i = 0; i < kShiftItems; ++i) {
+    const int slot = blockIdx.y * kShiftItems + i;
+    const int64_t r0 = sampled * slot / kShiftSplit, r1 = sampled * (slot + 1) / kShiftSplit;
+    double sum = 0.0, cnt = 0.0;
+    float lo = INFINITY, hi = -INFINITY;
+#pragma unroll
+    for (int k = 0; k < kShiftHeld; ++k) {
+      if (valid & (1u << (i * kShiftHeld + k))) {
+        const float v = held[i][k];
+        if (t.center_mean) {
+          sum += static_cast<double>(v);
+          cnt += 1.0;
+        }
+        lo = fminf(lo, v);
+        hi = fmaxf(hi, v);
+      }
+    }
+    // runs past the held ones (slots of more than kRowGroups * kShiftHeld runs)
+    for (int64_t run = r0 + row + kRowGroups * kShiftHeld; run < r1; run += kRowGroups) {
+      const int64_t px = run * step * 64 + col;
+      if (px < pixels) {
+        const float v = static_cast<float>(plane[px]);
+        if (t.center_mean) {
+          sum += static_cast<double>(v);
+          cnt += 1.0;
+        }
+        lo = fminf(lo, v);
+        hi = fmaxf(hi, v);
+      }
+    }
+    fold_subsample(sum, cnt, lo, hi, F.state, b, slot);
+  }
 }
 
 // One block per frame: r = the caller's reference, else the midpoint of the
@@ -1297,7 +1343,8 @@ FrameStats frame_of_job(const hsi_moments_job& j) {
 template <typename T>
 void launch_shift(const FrameTable& t, cudaStream_t s) {
   shift_init_kernel<<<t.n, 256, 0, s>>>(t);
-  shift_partial_kernel<T><<<dim3(t.max_bands, kShiftSplit, t.n), 256, 0, s>>>(t);
+  static_assert(kShiftSplit % kShiftItems == 0, "whole slots per block");
+  shift_partial_kernel<T><<<dim3(t.max_bands, kShiftSplit / kShiftItems, t.n), 256, 0, s>>>(t);
   shift_finalize_kernel<<<t.n, 256, 0, s>>>(t);
 }
 
