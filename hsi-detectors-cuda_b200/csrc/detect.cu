@@ -13,7 +13,11 @@
 //              then lower linear index).  Out-of-frame neighbours are NaN,
 //              which never win or tie, exactly like the bounds checks of the
 //              CPU loop.  Radii above 8 read each candidate's window from
-//              global memory instead;
+//              global memory instead.  Maps of radius <= 4 whose width is a
+//              multiple of 4 (and whose rows therefore start on 16 bytes)
+//              take a second kernel with the same steps over 512-column
+//              tiles: four columns per thread, 16-byte copies, polarity
+//              fixed at compile time;
 //   2. scan:   one block per map counts each row segment's passing pixels
 //              (popcounts of its mask words), turns the counts into output
 //              offsets starting at the caller's *count, and advances *count;
@@ -43,6 +47,14 @@ constexpr int kRing = 32;                          // ring rows (a power of two 
 static_assert(kRing >= 2 * kMaxRingR + 2 + kAhead, "ring too small for the window");
 constexpr int kRingCols = kTileW + 2 * kMaxRingR;  // 272
 constexpr int kFlagThreads = 288;                  // >= kRingCols, whole warps
+// fast flags tiles (radius <= kFastR, width a multiple of 4)
+constexpr int kFastW = 512;                        // columns per tile, four per candidate thread
+constexpr int kFastR = 4;                          // largest radius; also the halo of a ring row
+constexpr int kFastGroups = kFastW / 4 + 2;        // float4 groups of a ring row (one halo group each side)
+constexpr int kFastAhead = 6;                      // rows in flight ahead of the window
+constexpr int kFastRing = 16;                      // ring rows
+static_assert(kFastRing >= 2 * kFastR + kFastAhead + 2, "fast ring too small for the window");
+constexpr int kFastThreads = 160;                  // >= kFastGroups, whole warps
 
 struct Job {
   const float* score;
@@ -56,15 +68,17 @@ struct Job {
   uint32_t* count;
   int seg0;          // first segment of this map in the batch
   int segs_per_row;  // ceil(width / kSeg)
-  int tile0;         // first flags tile of this map in the batch
-  int tiles_x;       // ceil(width / kTileW)
+  int tile0;         // first flags tile of this map among the maps of its kind
+  int tiles_x;       // ceil(width / tile width of its kind)
 };
 
 struct Batch {
   Job jobs[kMaxJobs];
   int njobs;
   int total_segs;
-  int total_tiles;
+  int kind_jobs[2][kMaxJobs];  // job indices of the plain (0) and fast (1) flags kinds, in batch order
+  int kind_n[2];
+  int kind_tiles[2];
   uint32_t* counts;   // [total_segs]
   uint32_t* offsets;  // [total_segs]
   uint32_t* masks;    // [total_segs * 64]
@@ -79,13 +93,14 @@ __device__ __forceinline__ int find_job(const Batch& b, int seg) {
   return lo;
 }
 
-__device__ __forceinline__ int find_job_tile(const Batch& b, int tile) {
-  int lo = 0, hi = b.njobs - 1;
+// Job of flags tile `tile` of kind `kind` (0 plain, 1 fast).
+__device__ __forceinline__ int find_job_tile(const Batch& b, int kind, int tile) {
+  int lo = 0, hi = b.kind_n[kind] - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (b.jobs[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
+    if (b.jobs[b.kind_jobs[kind][mid]].tile0 <= tile) lo = mid; else hi = mid - 1;
   }
-  return lo;
+  return b.kind_jobs[kind][lo];
 }
 
 __device__ __forceinline__ bool better(float a, float b, bool higher) { return higher ? a > b : a < b; }
@@ -101,6 +116,9 @@ __device__ __forceinline__ uint32_t* mask_word(const Batch& b, const Job& J, int
 
 __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -232,9 +250,9 @@ __device__ void flags_tile_global(const Batch& b, const Job& J, int x0, int y0, 
 
 __global__ void __launch_bounds__(kFlagThreads) flags_kernel(const __grid_constant__ Batch b) {
   __shared__ FlagsSmem sm;
-  for (int tile = blockIdx.x; tile < b.total_tiles; tile += gridDim.x) {
+  for (int tile = blockIdx.x; tile < b.kind_tiles[0]; tile += gridDim.x) {
     __syncthreads();  // the previous tile is done with the shared buffers
-    const Job& J = b.jobs[find_job_tile(b, tile)];
+    const Job& J = b.jobs[find_job_tile(b, 0, tile)];
     const int local = tile - J.tile0;
     const int x0 = (local % J.tiles_x) * kTileW;
     const int y0 = (local / J.tiles_x) * kTileH;
@@ -251,6 +269,159 @@ __global__ void __launch_bounds__(kFlagThreads) flags_kernel(const __grid_consta
       case 8: flags_tile<8>(b, J, sm, x0, y0, y1); break;
       default: flags_tile_global(b, J, x0, y0, y1); break;
     }
+  }
+}
+
+// Shared memory of one fast flags tile: ring rows as float4 groups starting
+// kFastR columns left of the tile, and per group the column bests of the
+// window (score, row 0 .. 2r) for two consecutive rows.
+struct FastSmem {
+  float4 ring[kFastRing][kFastGroups];
+  float4 bv[2][kFastGroups];
+  int4 bk[2][kFastGroups];
+};
+
+template <bool HIGHER>
+__device__ __forceinline__ bool better_t(float a, float b) { return HIGHER ? a > b : a < b; }
+
+// Column c's first-best update with the value v of window row k (NaN never
+// wins; the first non-NaN value always does).
+template <bool HIGHER>
+__device__ __forceinline__ void best_update(float v, int k, float& bv, int& bk) {
+  if (!isnan(v) && (isnan(bv) || better_t<HIGHER>(v, bv))) {
+    bv = v;
+    bk = k;
+  }
+}
+
+// Bits 0..7 of x moved to bits 0, 4, .., 28.
+__device__ __forceinline__ uint32_t spread4(uint32_t x) {
+  x = (x | (x << 12)) & 0x000F000Fu;
+  x = (x | (x << 6)) & 0x03030303u;
+  x = (x | (x << 3)) & 0x11111111u;
+  return x;
+}
+
+// One fast tile: the steps of flags_tile with four adjacent columns per
+// thread.  Thread g < kFastGroups copies and reduces ring group g (columns
+// x0 - kFastR + 4g ..); thread t < kFastW / 4 judges columns x0 + 4t .. + 3,
+// whose windows lie in groups t .. t + 2.  The width is a multiple of 4, so
+// a group lies wholly inside or wholly outside the frame.
+template <int R, bool HIGHER>
+__device__ __forceinline__ void flags_fast_tile(const Batch& b, const Job& J, FastSmem& sm, int x0, int y0, int y1) {
+  static_assert(R <= kFastR, "radius above the fast halo");
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const float nan = __int_as_float(0x7fc00000);
+  const float4 nan4 = make_float4(nan, nan, nan, nan);
+  const int W = J.width, H = J.height;
+  const float thr = J.threshold;
+  const bool loader = t < kFastGroups;
+  const int gx = x0 - kFastR + 4 * t;  // first column of this thread's group
+  const bool col_in = loader && gx >= 0 && gx < W;
+  const int last = y1 - 1 + R;  // last row the tile reads
+  int next_row = y0 - R;
+  auto issue_next = [&]() {
+    if (next_row <= last && loader) {
+      float4* dst = &sm.ring[next_row & (kFastRing - 1)][t];
+      if (col_in && next_row >= 0 && next_row < H)
+        cp_async16(dst, J.score + static_cast<int64_t>(next_row) * W + gx);
+      else
+        *dst = nan4;
+    }
+    cp_async_commit();
+    ++next_row;
+  };
+#pragma unroll
+  for (int k = 0; k < 2 * R + kFastAhead; ++k) issue_next();
+  for (int y = y0; y <= y1; ++y) {
+    // row y + R + kFastAhead reuses the slot of row y + R + kFastAhead -
+    // kFastRing <= y - R - 2; the rows still read are y - 1 - R and later
+    if (y < y1) issue_next();
+    cp_async_wait<kFastAhead>();  // this thread's copies up to row y + R have landed
+    __syncthreads();              // ... and everyone's
+    if (y > y0 && t < kFastW / 4) {
+      // candidates of row y - 1 (its scores are still in the ring) against
+      // the column bests around them
+      const int yh = y - 1, hb = yh & 1;
+      const float4 c4 = sm.ring[yh & (kFastRing - 1)][t + 1];
+      const float s[4] = {c4.x, c4.y, c4.z, c4.w};
+      float v[12];
+      int k[12];
+#pragma unroll
+      for (int g = 0; g < 3; ++g) {
+        const float4 a = sm.bv[hb][t + g];
+        const int4 q = sm.bk[hb][t + g];
+        v[4 * g] = a.x; v[4 * g + 1] = a.y; v[4 * g + 2] = a.z; v[4 * g + 3] = a.w;
+        k[4 * g] = q.x; k[4 * g + 1] = q.y; k[4 * g + 2] = q.z; k[4 * g + 3] = q.w;
+      }
+      const bool in = x0 + 4 * t < W;
+      uint32_t word[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        bool pass = in && (HIGHER ? s[j] >= thr : s[j] <= thr);  // NaN fails both
+#pragma unroll
+        for (int dx = -R; dx <= R; ++dx) {
+          const int o = kFastR + j + dx;
+          // first in the window's order: better score, or the same score at
+          // a lower linear index (an earlier row, or this row to the left)
+          const bool earlier = dx < 0 ? k[o] <= R : k[o] < R;
+          if (better_t<HIGHER>(v[o], s[j]) || (v[o] == s[j] && earlier)) pass = false;
+        }
+        word[j] = __ballot_sync(0xffffffffu, pass);  // bit l: column 4l + j of the warp's 128
+      }
+      if (lane < 4) {
+        // mask word `lane` of the warp: its columns 32 lane + 4i + j come
+        // from bit 8 lane + i of word[j]
+        uint32_t m = 0u;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) m |= spread4((word[j] >> (8 * lane)) & 0xffu) << j;
+        const int xw = x0 + 128 * warp + 32 * lane;
+        if (xw < W) *mask_word(b, J, yh, xw) = m;
+      }
+    }
+    if (y < y1 && loader) {
+      // group t's column first-bests over rows y - R .. y + R
+      float4 bv = nan4;
+      int4 bk = make_int4(0, 0, 0, 0);
+#pragma unroll
+      for (int k = 0; k <= 2 * R; ++k) {
+        const float4 a = sm.ring[(y - R + k) & (kFastRing - 1)][t];
+        best_update<HIGHER>(a.x, k, bv.x, bk.x);
+        best_update<HIGHER>(a.y, k, bv.y, bk.y);
+        best_update<HIGHER>(a.z, k, bv.z, bk.z);
+        best_update<HIGHER>(a.w, k, bv.w, bk.w);
+      }
+      sm.bv[y & 1][t] = bv;
+      sm.bk[y & 1][t] = bk;
+    }
+  }
+}
+
+template <bool HIGHER>
+__device__ __forceinline__ void flags_fast_dispatch(const Batch& b, const Job& J, FastSmem& sm, int x0, int y0,
+                                                    int y1) {
+  switch (J.radius > 0 ? J.radius : 0) {
+    case 0: flags_fast_tile<0, HIGHER>(b, J, sm, x0, y0, y1); break;
+    case 1: flags_fast_tile<1, HIGHER>(b, J, sm, x0, y0, y1); break;
+    case 2: flags_fast_tile<2, HIGHER>(b, J, sm, x0, y0, y1); break;
+    case 3: flags_fast_tile<3, HIGHER>(b, J, sm, x0, y0, y1); break;
+    default: flags_fast_tile<4, HIGHER>(b, J, sm, x0, y0, y1); break;  // the host admits radius <= kFastR only
+  }
+}
+
+__global__ void __launch_bounds__(kFastThreads) flags_fast_kernel(const __grid_constant__ Batch b) {
+  __shared__ FastSmem sm;
+  for (int tile = blockIdx.x; tile < b.kind_tiles[1]; tile += gridDim.x) {
+    __syncthreads();  // the previous tile is done with the shared buffers
+    const Job& J = b.jobs[find_job_tile(b, 1, tile)];
+    const int local = tile - J.tile0;
+    const int x0 = (local % J.tiles_x) * kFastW;
+    const int y0 = (local / J.tiles_x) * kTileH;
+    const int y1 = min(J.height, y0 + kTileH);
+    if (J.higher)
+      flags_fast_dispatch<true>(b, J, sm, x0, y0, y1);
+    else
+      flags_fast_dispatch<false>(b, J, sm, x0, y0, y1);
   }
 }
 
@@ -387,7 +558,7 @@ int sm_count() {
 int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cudaStream_t s) {
   if (!jobs || n <= 0 || n > kMaxJobs) return HSI_E_INVALID;
   Batch b{};
-  int64_t segs = 0, tiles = 0;
+  int64_t segs = 0, tiles[2] = {0, 0};
   for (int i = 0; i < n; ++i) {
     const hsi_detect_job& j = jobs[i];
     if (!j.score || !j.count || j.height <= 0 || j.width <= 0 || j.capacity < 0) return HSI_E_INVALID;
@@ -406,32 +577,48 @@ int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cuda
     J.count = j.count;
     J.seg0 = static_cast<int>(segs);
     J.segs_per_row = (j.width + kSeg - 1) / kSeg;
-    J.tile0 = static_cast<int>(tiles);
-    J.tiles_x = (j.width + kTileW - 1) / kTileW;
+    // fast flags tiles: radius <= kFastR and rows that start on 16 bytes
+    const int kind = j.nms_radius <= kFastR && j.width % 4 == 0 &&
+                     (reinterpret_cast<uintptr_t>(j.score) & 15u) == 0;
+    const int tile_w = kind ? kFastW : kTileW;
+    J.tile0 = static_cast<int>(tiles[kind]);
+    J.tiles_x = (j.width + tile_w - 1) / tile_w;
+    b.kind_jobs[kind][b.kind_n[kind]++] = i;
     segs += segs_of(j.height, j.width);
-    tiles += static_cast<int64_t>(J.tiles_x) * ((j.height + kTileH - 1) / kTileH);
-    if (segs > 0x3fffffff || tiles > 0x3fffffff) return HSI_E_CAPACITY;
+    tiles[kind] += static_cast<int64_t>(J.tiles_x) * ((j.height + kTileH - 1) / kTileH);
+    if (segs > 0x3fffffff || tiles[kind] > 0x3fffffff) return HSI_E_CAPACITY;
   }
   if (!ws || ws_bytes < ws_bytes_for_segs(segs)) return HSI_E_WORKSPACE;
   if ((reinterpret_cast<uintptr_t>(ws) & 15u) != 0) return HSI_E_INVALID;
   b.njobs = n;
   b.total_segs = static_cast<int>(segs);
-  b.total_tiles = static_cast<int>(tiles);
+  b.kind_tiles[0] = static_cast<int>(tiles[0]);
+  b.kind_tiles[1] = static_cast<int>(tiles[1]);
   uint32_t* p = static_cast<uint32_t*>(ws);
   b.counts = p;
   b.offsets = p + segs;
   b.masks = p + 2 * segs;
-  // one wave of resident tiles (30 KB of shared memory, 288 threads each)
-  static int per_sm = 0;
-  if (per_sm == 0) {
+  // one wave of resident tiles per flags kind (41 KB of shared memory each)
+  static int per_sm[2] = {0, 0};
+  if (per_sm[0] == 0) {
     int v = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, flags_kernel, kFlagThreads, 0) != cudaSuccess || v <= 0) v = 4;
-    per_sm = v;
+    per_sm[0] = v;
+    v = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, flags_fast_kernel, kFastThreads, 0) != cudaSuccess || v <= 0)
+      v = 4;
+    per_sm[1] = v;
   }
-  const int64_t wave = static_cast<int64_t>(per_sm) * sm_count();
-  const int flag_grid = static_cast<int>(tiles < wave ? tiles : wave);
   const int grid = static_cast<int>(segs < 16 * sm_count() ? segs : 16 * sm_count());
-  flags_kernel<<<flag_grid, kFlagThreads, 0, s>>>(b);
+  for (int kind = 0; kind < 2; ++kind) {
+    if (tiles[kind] == 0) continue;
+    const int64_t wave = static_cast<int64_t>(per_sm[kind]) * sm_count();
+    const int flag_grid = static_cast<int>(tiles[kind] < wave ? tiles[kind] : wave);
+    if (kind == 0)
+      flags_kernel<<<flag_grid, kFlagThreads, 0, s>>>(b);
+    else
+      flags_fast_kernel<<<flag_grid, kFastThreads, 0, s>>>(b);
+  }
   scan_kernel<<<n, 1024, 0, s>>>(b);
   emit_kernel<<<grid, kThreads, 0, s>>>(b);
   return static_cast<int>(cudaGetLastError());
