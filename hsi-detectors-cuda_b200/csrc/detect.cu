@@ -22,7 +22,8 @@
 //              (popcounts of its mask words), turns the counts into output
 //              offsets starting at the caller's *count, and advances *count;
 //   3. emit:   each segment writes its detections at offset + in-segment
-//              rank, dropping (but having counted) those past capacity.
+//              rank, dropping (but having counted) those past capacity;
+//              segments whose count is zero cost one load.
 // Semantics are the reference CPU path's (src/sam_cpu.cpp:86-138), polarity
 // included; the reference GPU kernel (src/detect.cu:43-87) ignores polarity
 // and emits in atomic arrival order, both of which this replaces.
@@ -494,6 +495,7 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(const __grid_constant__ 
   __shared__ uint32_t s_prefix[kWordsPerSeg];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int seg = blockIdx.x; seg < b.total_segs; seg += gridDim.x) {
+    if (b.counts[seg] == 0u) continue;  // nothing passed in this segment (the same for the whole block)
     __syncthreads();
     const Job& J = b.jobs[find_job(b, seg)];
     const int local = seg - J.seg0;
