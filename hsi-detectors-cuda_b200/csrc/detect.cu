@@ -21,9 +21,9 @@
 //   2. scan:   one block per map counts each row segment's passing pixels
 //              (popcounts of its mask words), turns the counts into output
 //              offsets starting at the caller's *count, and advances *count;
-//   3. emit:   each segment writes its detections at offset + in-segment
-//              rank, dropping (but having counted) those past capacity;
-//              segments whose count is zero cost one load.
+//   3. emit:   one warp per segment writes its detections at offset +
+//              in-segment rank, dropping (but having counted) those past
+//              capacity; segments whose count is zero cost one load.
 // Semantics are the reference CPU path's (src/sam_cpu.cpp:86-138), polarity
 // included; the reference GPU kernel (src/detect.cu:43-87) ignores polarity
 // and emits in atomic arrival order, both of which this replaces.
@@ -490,52 +490,60 @@ __global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ Batc
   if (threadIdx.x == 0) *J.count = s_carry;
 }
 
+// One warp per segment.  Lane l holds mask words l and l + 32, their
+// exclusive prefix of popcounts comes from two shuffle scans, and the warp
+// then visits the non-empty words in order with lane = bit, so that the
+// detections of one word go to consecutive slots in one coalesced store.
 __global__ void __launch_bounds__(kThreads) emit_kernel(const __grid_constant__ Batch b) {
-  __shared__ uint32_t s_words[kWordsPerSeg];
-  __shared__ uint32_t s_prefix[kWordsPerSeg];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int seg = blockIdx.x; seg < b.total_segs; seg += gridDim.x) {
-    if (b.counts[seg] == 0u) continue;  // nothing passed in this segment (the same for the whole block)
-    __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (kThreads / 32);
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int seg = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); seg < b.total_segs; seg += warps) {
+    const uint32_t count = b.counts[seg];
+    if (count == 0u) continue;  // nothing passed in this segment (the same for the whole warp)
     const Job& J = b.jobs[find_job(b, seg)];
     const int local = seg - J.seg0;
-    if (threadIdx.x < kWordsPerSeg)
-      s_words[threadIdx.x] = static_cast<int>(threadIdx.x) < seg_words(J, local)
-                                 ? b.masks[static_cast<int64_t>(seg) * kWordsPerSeg + threadIdx.x]
-                                 : 0u;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      const uint32_t a = __popc(s_words[2 * lane]), c = __popc(s_words[2 * lane + 1]);
-      uint32_t incl = a + c;
+    const int nw = seg_words(J, local);
+    const uint32_t* m = b.masks + static_cast<int64_t>(seg) * kWordsPerSeg;
+    const uint32_t w0 = lane < nw ? m[lane] : 0u;
+    const uint32_t w1 = lane + 32 < nw ? m[lane + 32] : 0u;
+    const uint32_t base = b.offsets[seg];
+    const uint32_t c0 = __popc(w0), c1 = __popc(w1);
+    uint32_t i0 = c0, i1 = c1;  // inclusive scans over the lanes
 #pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= d) incl += o;
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o0 = __shfl_up_sync(0xffffffffu, i0, d);
+      const uint32_t o1 = __shfl_up_sync(0xffffffffu, i1, d);
+      if (lane >= d) {
+        i0 += o0;
+        i1 += o1;
       }
-      const uint32_t excl = incl - a - c;
-      s_prefix[2 * lane] = excl;
-      s_prefix[2 * lane + 1] = excl + a;
     }
-    __syncthreads();
+    const uint32_t first_half = __shfl_sync(0xffffffffu, i0, 31);
+    const uint32_t e0 = i0 - c0, e1 = first_half + i1 - c1;  // exclusive prefixes of words lane, lane + 32
     const int y = local / J.segs_per_row;
     const int x0 = (local % J.segs_per_row) * kSeg;
-    const uint32_t base = b.offsets[seg];
-    const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
-    for (int i = 0; i < kPerThread; ++i) {
-      const int w = i * (kThreads / 32) + warp;
-      const uint32_t word = s_words[w];
-      if ((word >> lane) & 1u) {
-        const uint32_t slot = base + s_prefix[w] + __popc(word & lt);
-        if (slot < static_cast<uint32_t>(J.capacity)) {
-          const int x = x0 + w * 32 + lane;
-          const int64_t p = static_cast<int64_t>(y) * J.width + x;
-          hsi_detection d;
-          d.x = x;
-          d.y = y;
-          d.target = J.target ? J.target[p] : 0;
-          d.score = J.score[p];
-          J.out[slot] = d;
+    for (int half = 0; half < 2; ++half) {
+      const uint32_t mine = half ? w1 : w0, pre = half ? e1 : e0;
+      uint32_t nonempty = __ballot_sync(0xffffffffu, mine != 0u);
+      while (nonempty) {
+        const int wi = __ffs(nonempty) - 1;
+        nonempty &= nonempty - 1u;
+        const uint32_t word = __shfl_sync(0xffffffffu, mine, wi);
+        const uint32_t wpre = __shfl_sync(0xffffffffu, pre, wi);
+        if ((word >> lane) & 1u) {
+          const uint32_t slot = base + wpre + __popc(word & lt);
+          if (slot < static_cast<uint32_t>(J.capacity)) {
+            const int x = x0 + (32 * half + wi) * 32 + lane;
+            const int64_t p = static_cast<int64_t>(y) * J.width + x;
+            hsi_detection d;
+            d.x = x;
+            d.y = y;
+            d.target = J.target ? J.target[p] : 0;
+            d.score = J.score[p];
+            J.out[slot] = d;
+          }
         }
       }
     }
@@ -611,7 +619,8 @@ int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cuda
       v = 4;
     per_sm[1] = v;
   }
-  const int grid = static_cast<int>(segs < 16 * sm_count() ? segs : 16 * sm_count());
+  const int64_t emit_blocks = (segs + kThreads / 32 - 1) / (kThreads / 32);  // a warp per segment
+  const int grid = static_cast<int>(emit_blocks < 16 * sm_count() ? emit_blocks : 16 * sm_count());
   for (int kind = 0; kind < 2; ++kind) {
     if (tiles[kind] == 0) continue;
     const int64_t wave = static_cast<int64_t>(per_sm[kind]) * sm_count();
