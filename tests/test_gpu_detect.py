@@ -142,3 +142,43 @@ def test_batched_maps_match_single_calls(hsi, orc):
         n, got = hsi.detections_to_numpy(count, out, H * W + 1)
         assert n == n0
         assert _tuples(got) == _tuples(want)
+
+
+@pytest.mark.parametrize("shape", [(1, 4), (3, 508), (65, 512), (66, 516), (129, 1028)])
+@pytest.mark.parametrize("radius", [-1, 3, 4, 5])
+@pytest.mark.parametrize("higher", [False, True])
+def test_tile_edges_and_kernel_switch_bit_exact(hsi, orc, shape, radius, higher):
+    """Widths that are multiples of 4 around the 512-column tiles and 64-row bands of the
+    four-column flags kernel, at radii on both sides of its limit (4; 5 takes the plain
+    kernel), with NaN scores and quantised ties."""
+    H, W = shape
+    rng = np.random.default_rng(H * 131 + W * 7 + radius + 3)
+    score = (rng.integers(0, 25, H * W) / 25.0).astype(np.float32)
+    score[rng.integers(0, H * W, max(1, H * W // 40))] = np.nan
+    target = rng.integers(0, 8, H * W).astype(np.int32)
+    thr = 0.88 if higher else 0.12
+    n0, want = orc.detect(score, target, H, W, thr, radius, higher, capacity=1 << 22)
+    n, got = _gpu_detect(hsi, score, target, H, W, thr, radius, higher)
+    assert n == n0
+    assert _tuples(got) == _tuples(want)
+
+
+def test_unaligned_map_takes_the_plain_kernel(hsi, orc):
+    """A map that does not start on 16 bytes runs the plain flags kernel, with the same result."""
+    H, W, r = 70, 260, 2
+    rng = np.random.default_rng(91)
+    score = (rng.integers(0, 25, H * W) / 25.0).astype(np.float32)
+    target = rng.integers(0, 8, H * W).astype(np.int32)
+    buf = torch.zeros(H * W + 4, device="cuda")
+    buf[1:1 + H * W] = torch.from_numpy(score).cuda()
+    s = buf[1:1 + H * W]
+    assert s.data_ptr() % 16 == 4
+    t = torch.from_numpy(target).cuda()
+    for higher in (False, True):
+        thr = 0.88 if higher else 0.12
+        n0, want = orc.detect(score, target, H, W, thr, r, higher, capacity=1 << 16)
+        cnt, out = hsi.detect(s, t, H, W, thr, r, 1 if higher else 0, 1 << 16)
+        torch.cuda.synchronize()
+        n, got = hsi.detections_to_numpy(cnt, out, 1 << 16)
+        assert n == n0
+        assert _tuples(got) == _tuples(want)
