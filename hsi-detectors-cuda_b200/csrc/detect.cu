@@ -305,7 +305,7 @@ __device__ __forceinline__ uint32_t spread4(uint32_t x) {
 
 // One fast tile: the steps of flags_tile with four adjacent columns per
 // thread.  Thread g < kFastGroups copies and reduces ring group g (columns
-// x0 - kFastR + 4g ..); thread t < kFastW / 4 judges columns x0 + 4t .. + 3,
+// x0 - kFastR + 4g ..); thread t < kFastW / 4 tests columns x0 + 4t .. + 3,
 // whose windows lie in groups t .. t + 2.  The width is a multiple of 4, so
 // a group lies wholly inside or wholly outside the frame.
 template <int R, bool HIGHER>
