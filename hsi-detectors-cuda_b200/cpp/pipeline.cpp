@@ -23,7 +23,7 @@ bool parse_memory_mode(const std::string& name, MemoryMode* out) {
     *out = MemoryMode::Copy;
     return true;
   }
-  if (name == "zerocopy") {
+  if (name == "zerocopy" || name == "zero-copy") {  // the reference's alias (src/pipeline.cu:452-456)
     *out = MemoryMode::ZeroCopy;
     return true;
   }

@@ -18,19 +18,25 @@ constexpr int kMaxTargets = 64;
 const char* to_string(SamVariant variant) {
   switch (variant) {
     case SamVariant::Baseline: return "baseline";
-    case SamVariant::Optimized: return "opt";
+    case SamVariant::Optimized: return "optimized";
     case SamVariant::Half: return "half";
     case SamVariant::BipDirect: return "bip";
   }
   return "unknown";
 }
 
+// The reference's names and aliases (src/sam.cu:330-336): "opt" and "fp16"
+// are accepted beside the names to_string gives.
 bool parse_sam_variant(const std::string& name, SamVariant* out) {
   for (SamVariant v : {SamVariant::Baseline, SamVariant::Optimized, SamVariant::Half, SamVariant::BipDirect}) {
     if (name == to_string(v)) {
       *out = v;
       return true;
     }
+  }
+  if (name == "opt" || name == "fp16") {
+    *out = name == "opt" ? SamVariant::Optimized : SamVariant::Half;
+    return true;
   }
   return false;
 }

@@ -25,7 +25,7 @@ REFERENCE_NAMES = [
     "hsi::moment_cube_reads(", "hsi::build_statistics(", "hsi::traits_of(", "hsi::parse_detector(",
     "hsi::rx_threshold_for_false_alarm_rate(", "hsi::Pipeline::create(", "hsi::make_synthetic_source(",
     "hsi::moments_from_shifted(", "hsi::SpectralLibrary::flatten(", "hsi::SpectralLibrary::norms(",
-    "hsi::convert_interleave(", "hsi::parse_memory_mode(",
+    "hsi::convert_interleave(", "hsi::parse_memory_mode(", "hsi::read_spectra_csv(", "hsi::write_spectra_csv(",
 ]
 
 
@@ -45,6 +45,14 @@ def test_cpp_library_exports_the_reference_entry_points():
     out = subprocess.run(["nm", "-DC", "--defined-only", CXXLIB], check=True, capture_output=True, text=True).stdout
     missing = [n for n in REFERENCE_NAMES if n not in out]
     assert not missing, missing
+
+
+def test_host_only_program_passes_without_a_device():
+    """Name parsers and the CSV library reader: no device calls."""
+    _make_tests()
+    r = subprocess.run([os.path.join(BIN, "test_host_api")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip().splitlines()[-1] == "ok host_api", r.stdout
 
 
 @pytest.mark.gpu
