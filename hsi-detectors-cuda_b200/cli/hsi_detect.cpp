@@ -20,8 +20,8 @@
 //   --loading=F                diagonal loading of the statistics
 //   --autotune                 time the batch runner's choices on the batch
 // Flags are checked before the device is touched, so a usage error exits 2
-// on any machine.  Frame sources other than the synthetic one (ENVI replay,
-// HOT snapshot mosaics) are not built: they exit 2 with that message.
+// on any machine.  Sources: synthetic, and ENVI replay (--envi, --resident);
+// the HOT snapshot-mosaic directory source is not built and exits 2.
 #include <algorithm>
 #include <chrono>
 #include <cstdint>
@@ -53,8 +53,10 @@ const char* kUsage = R"(hsi_detect - hyperspectral target detection (SAM, CEM, R
   hsi_detect [options]
 
 Source
-  --source=synthetic            where frames come from            [synthetic]
-                                (envi and hot are not built here)
+  --source=synthetic|envi       where frames come from            [synthetic]
+                                (hot is not built here)
+  --envi=A.hdr,B.hdr            ENVI cubes to replay
+  --resident=N                  cubes held in RAM                         [4]
   --width=N --height=N          synthetic frame size               [512x512]
   --bands=N                     synthetic band count                    [128]
   --targets=N                   synthetic planted targets                 [3]
@@ -150,6 +152,8 @@ double real(const Args& a, const std::string& key, double fallback) {
 
 struct Config {
   hsi::SyntheticOptions synthetic;
+  bool envi = false;
+  hsi::EnviReplayOptions replay;
   hsi::Detector detector = hsi::Detector::Sam;
   std::string library_path;
   bool threshold_given = false;
@@ -166,9 +170,20 @@ struct Config {
 Config configure(const Args& a) {
   Config c;
   const std::string source = a.str("source", "synthetic");
-  if (source == "envi" || source == "hot")
-    throw UsageError{"--source=" + source + " is not built in this library; use --source=synthetic"};
-  if (source != "synthetic") throw UsageError{"unknown --source=" + source};
+  if (source == "hot") throw UsageError{"--source=hot is not built in this library; use synthetic or envi"};
+  if (source != "synthetic" && source != "envi") throw UsageError{"unknown --source=" + source};
+  if (source == "envi") {
+    c.envi = true;
+    const std::string list = a.str("envi", "");
+    std::size_t start = 0;
+    while (start <= list.size()) {
+      const std::size_t comma = std::min(list.find(',', start), list.size());
+      if (comma > start) c.replay.hdr_paths.push_back(list.substr(start, comma - start));
+      start = comma + 1;
+    }
+    if (c.replay.hdr_paths.empty()) throw UsageError{"--source=envi needs --envi=<header>[,<header>...]"};
+    c.replay.max_resident = integer(a, "resident", 4, 1, 1 << 16);
+  }
   c.synthetic.shape.height = integer(a, "height", 512, 1, 1 << 16);
   c.synthetic.shape.width = integer(a, "width", 512, 1, 1 << 16);
   c.synthetic.shape.bands = integer(a, "bands", 128, 1, 256);
@@ -645,13 +660,14 @@ int main(int argc, char** argv) {
     hsi::SpectralLibrary library;
     std::unique_ptr<hsi::FrameSource> source;
     if (!c.library_path.empty()) library = hsi::read_spectra_csv(c.library_path);
-    source = hsi::make_synthetic_source(c.synthetic);
+    source = c.envi ? hsi::make_envi_replay_source(c.replay) : hsi::make_synthetic_source(c.synthetic);
     if (!source) {
-      std::fprintf(stderr, "pipeline setup failed: synthetic source\n");
+      std::fprintf(stderr, "pipeline setup failed: frame source\n");
       return 1;
     }
     if (c.library_path.empty()) {
-      // the synthetic source knows what it planted, so the tool runs with no arguments at all
+      // the synthetic source knows what it planted, so the tool runs with no
+      // arguments at all; an ENVI replay needs --library
       if (!source->library()) {
         std::fputs("no target spectra: pass --library=<csv>\n", stderr);
         return 2;

@@ -57,4 +57,17 @@ struct SyntheticOptions {
 };
 std::unique_ptr<FrameSource> make_synthetic_source(const SyntheticOptions& options);
 
+// ENVI cubes replayed from disk (reference include/hsi/frame_source.hpp:60-69):
+// the first max(1, max_resident) headers are read (read_envi, as BSQ) when the
+// source is made, all of the first cube's shape, and frames cycle through them
+// (or end after the last when !loop).  Frame i has index i and timestamp i / 30 s.
+// Throws std::invalid_argument with no headers, std::runtime_error when a cube
+// cannot be read or its shape differs from the first.
+struct EnviReplayOptions {
+  std::vector<std::string> hdr_paths;
+  int max_resident = 4;
+  bool loop = true;
+};
+std::unique_ptr<FrameSource> make_envi_replay_source(const EnviReplayOptions& options);
+
 }  // namespace hsi

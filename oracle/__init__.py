@@ -147,6 +147,8 @@ def ref_lib():
         lib.ref_frame_sam_cem.restype = i64
         lib.ref_frame_rx_ace.argtypes = [f32p, ci, ci, ci, f32p, ci, C.c_double, f32p, i32p, f32p]
         lib.ref_frame_rx_ace.restype = ci
+        lib.ref_read_envi.argtypes = [C.c_char_p, ci, i32p, f32p, i64, f32p, ci, C.c_char_p, ci]
+        lib.ref_read_envi.restype = ci
         _ref = lib
     return _ref
 
@@ -447,3 +449,23 @@ def mlp(params, bands, features, labels=None, pos_weight=1.0, round_bf16=True, g
     loss = fp64_lib().orc_mlp(_f(params), bands, _f(features), _f(lab), n, float(pos_weight),
                               1 if round_bf16 else 0, _d(logits), _d(g))
     return logits, loss, g
+
+
+def ref_read_envi(hdr_path, to=0):
+    """The reference's own read_envi (oracle/_ref): (cube (H, W, B) float32 in the
+    requested interleave's flat order, wavelengths) or raises RuntimeError with the
+    reference's message."""
+    lib = ref_lib()
+    dims = np.zeros(4, np.int32)
+    err = C.create_string_buffer(512)
+    empty = np.zeros(1, np.float32)
+    rc = lib.ref_read_envi(hdr_path.encode(), to, _i(dims), _f(empty), 0, _f(empty), 0, err, 512)
+    if rc == 1:
+        raise RuntimeError(err.value.decode())
+    n = int(dims[0]) * int(dims[1]) * int(dims[2])
+    data = np.zeros(max(n, 1), np.float32)
+    wl = np.zeros(max(int(dims[3]), 1), np.float32)
+    rc = lib.ref_read_envi(hdr_path.encode(), to, _i(dims), _f(data), n, _f(wl), int(dims[3]), err, 512)
+    if rc != 0:
+        raise RuntimeError(err.value.decode() if rc == 1 else "capacity")
+    return (int(dims[0]), int(dims[1]), int(dims[2])), data[:n], wl[:int(dims[3])]

@@ -17,6 +17,7 @@
 //   ref_moments_from_shifted        src/linalg.cpp:81-162
 //   ref_demosaic                    hsi::demosaic                       (src/hot_loader.cpp:144-182)
 //   ref_synthetic_frame             hsi::make_synthetic_source          (src/frame_source.cpp:149-293)
+//   ref_read_envi                   hsi::read_envi                      (src/envi.cpp:195-258)
 #include <cstdint>
 #include <cstring>
 #include <exception>
@@ -25,6 +26,7 @@
 
 #include "hsi/detector.hpp"
 #include "hsi/detectors.hpp"
+#include "hsi/envi.hpp"
 #include "hsi/frame_source.hpp"
 #include "hsi/hot_loader.hpp"
 #include "hsi/linalg.hpp"
@@ -307,4 +309,30 @@ REF_API int ref_frame_rx_ace(const float* cube, int h, int w, int b, const float
   if (!hsi::build_statistics(m, lib, loading, &s, &err)) return 0;
   hsi::ace_best_cpu(cube, shape, s, ace, ace_target, rx);
   return 1;
+}
+
+// The reference's read_envi of `hdr` into interleave `to` (0 BSQ, 1 BIL,
+// 2 BIP).  dims = {height, width, bands, wavelength count}.  Returns 0 with
+// data (capacity floats) and wavelengths (wl_capacity floats) filled, 2 when
+// a capacity is too small (dims filled), 1 on an exception, whose message
+// goes to err (err_len bytes, NUL-terminated).
+REF_API int ref_read_envi(const char* hdr, int to, int* dims, float* data, int64_t capacity, float* wavelengths,
+                          int wl_capacity, char* err, int err_len) {
+  try {
+    const hsi::HsiFrame f = hsi::read_envi(hdr, static_cast<hsi::Interleave>(to));
+    dims[0] = f.shape.height;
+    dims[1] = f.shape.width;
+    dims[2] = f.shape.bands;
+    dims[3] = static_cast<int>(f.wavelengths_nm.size());
+    if (static_cast<int64_t>(f.data.size()) > capacity || dims[3] > wl_capacity) return 2;
+    std::memcpy(data, f.data.data(), f.data.size() * sizeof(float));
+    if (dims[3]) std::memcpy(wavelengths, f.wavelengths_nm.data(), f.wavelengths_nm.size() * sizeof(float));
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) {
+      std::strncpy(err, e.what(), static_cast<std::size_t>(err_len) - 1);
+      err[err_len - 1] = '\0';
+    }
+    return 1;
+  }
 }

@@ -4,15 +4,21 @@
 //     (src/sam.cu:320-336, src/pipeline.cu:444-456, src/detector.cpp:21-45);
 //   * read_spectra_csv / write_spectra_csv follow the reference's CSV format
 //     and error cases (src/spectra_io.cpp:27-122), and a written library reads
-//     back bit for bit.
+//     back bit for bit;
+//   * make_envi_replay_source replays ENVI cubes as the reference's
+//     EnviReplaySource does (src/frame_source.cpp:69-145).
+#include <cstdint>
 #include <cstdio>
 #include <fstream>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "check.hpp"
 #include "hsi/detector.hpp"
+#include "hsi/envi.hpp"
+#include "hsi/frame_source.hpp"
 #include "hsi/pipeline.hpp"
 #include "hsi/sam_cuda.hpp"
 #include "hsi/spectra_io.hpp"
@@ -133,6 +139,76 @@ void test_library_round_trips_bit_for_bit() {
   }
 }
 
+// A height x width x bands f32 BIP cube whose value at (b, y, x) is
+// base + b * 1000 + y * 10 + x, written as <name>.hdr and <name>.
+std::string write_bip_cube(const char* name, int h, int w, int bands, float base) {
+  const std::string hdr = temp_path(name) + ".hdr";
+  std::ofstream(hdr) << "ENVI\nsamples = " << w << "\nlines = " << h << "\nbands = " << bands
+                     << "\ndata type = 4\ninterleave = bip\nbyte order = 0\n";
+  std::vector<float> v;
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x)
+      for (int b = 0; b < bands; ++b) v.push_back(base + b * 1000.0f + y * 10.0f + x);
+  std::ofstream(temp_path(name), std::ios::binary)
+      .write(reinterpret_cast<const char*>(v.data()), static_cast<std::streamsize>(v.size() * sizeof(float)));
+  return hdr;
+}
+
+void test_envi_replay_cycles_resident_cubes() {
+  const std::string a = write_bip_cube("replay_a", 3, 4, 2, 0.0f);
+  const std::string b = write_bip_cube("replay_b", 3, 4, 2, 0.5f);
+  const std::string c = write_bip_cube("replay_c", 3, 4, 2, 0.25f);
+  EnviReplayOptions o;
+  o.hdr_paths = {a, b, c};
+  o.max_resident = 2;  // the third cube is never read
+  o.loop = false;
+  std::unique_ptr<FrameSource> src = make_envi_replay_source(o);
+  CHECK(src->shape() == CubeShape({3, 4, 2}));
+  CHECK(src->interleave() == Interleave::Bsq);
+  CHECK(src->length() == 2);
+  CHECK(src->describe() == "envi-replay(2 cubes, 3x4x2)");
+  const std::size_t stride = 16;  // wider than the 12 pixels: planes land 16 floats apart
+  std::vector<float> dst(stride * 2, -1.0f);
+  FrameMeta meta;
+  for (int f = 0; f < 2; ++f) {
+    CHECK(src->read_into(dst.data(), stride, &meta));
+    CHECK(meta.index == static_cast<std::uint64_t>(f));
+    CHECK(meta.timestamp_s == f / 30.0);
+    const float base = f == 0 ? 0.0f : 0.5f;
+    for (int band = 0; band < 2; ++band)
+      for (int y = 0; y < 3; ++y)
+        for (int x = 0; x < 4; ++x) CHECK(dst[band * stride + y * 4 + x] == base + band * 1000.0f + y * 10.0f + x);
+    CHECK(dst[12] == -1.0f);  // the stride padding is left alone
+  }
+  CHECK(!src->read_into(dst.data(), stride, &meta));
+  src->reset();
+  CHECK(src->read_into(dst.data(), stride, &meta) && meta.index == 0 && dst[0] == 0.0f);
+  o.loop = true;
+  o.max_resident = 1;
+  std::unique_ptr<FrameSource> looped = make_envi_replay_source(o);
+  CHECK(looped->length() == 0);
+  for (int f = 0; f < 3; ++f) CHECK(looped->read_into(dst.data(), 12, &meta) && meta.index == static_cast<std::uint64_t>(f));
+}
+
+void test_envi_replay_rejects_what_the_reference_rejects() {
+  bool threw = false;
+  try {
+    make_envi_replay_source(EnviReplayOptions{});
+  } catch (const std::invalid_argument&) {
+    threw = true;
+  }
+  CHECK(threw);
+  EnviReplayOptions o;
+  o.hdr_paths = {write_bip_cube("shape_a", 3, 4, 2, 0.0f), write_bip_cube("shape_b", 3, 5, 2, 0.0f)};
+  std::string message;
+  try {
+    make_envi_replay_source(o);
+  } catch (const std::runtime_error& e) {
+    message = e.what();
+  }
+  CHECK(contains(message, "is 3x5x2, expected the shape of the first cube"));
+}
+
 }  // namespace
 
 int main() {
@@ -142,5 +218,7 @@ int main() {
   test_library_reads_the_reference_format();
   test_library_errors_name_the_file_and_line();
   test_library_round_trips_bit_for_bit();
+  test_envi_replay_cycles_resident_cubes();
+  test_envi_replay_rejects_what_the_reference_rejects();
   return tcheck::finish("host_api");
 }

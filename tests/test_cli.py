@@ -26,7 +26,7 @@ def test_help_lists_the_reference_flags_and_the_added_ones():
     _build()
     r = _run("--help")
     assert r.returncode == 0
-    for flag in ["--source=", "--width=", "--height=", "--bands=", "--targets=", "--noise=", "--library=",
+    for flag in ["--source=", "--envi=", "--resident=", "--width=", "--height=", "--bands=", "--targets=", "--noise=", "--library=",
                  "--threshold=", "--nms=", "--max-detections=", "--variant=", "--memory=", "--streams=",
                  "--frames=", "--warmup=", "--prefill", "--csv=", "--print-detections=", "--dump-score=",
                  "--quiet", "--detector=sam|cem|rx|ace", "--batch", "--repeat=", "--pfa=", "--loading="]:
@@ -34,7 +34,7 @@ def test_help_lists_the_reference_flags_and_the_added_ones():
 
 
 @pytest.mark.parametrize("args, message", [
-    (["--source=envi"], "not built in this library"),
+    (["--source=envi"], "--source=envi needs --envi=<header>[,<header>...]"),
     (["--source=hot"], "not built in this library"),
     (["--source=tape"], "unknown --source=tape"),
     (["--detector=mahalanobis"], "--detector must be sam, cem, rx or ace"),
@@ -82,3 +82,43 @@ def test_batch_mode_runs(detector):
              "--warmup=1", "--repeat=3", "--print-detections=2", timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "batch of 4 frames" in r.stdout, r.stdout
+
+
+def _envi_cube(tmp_path, name, H, W, B, seed):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    cube = rng.uniform(0.05, 1.0, (H, W, B)).astype("<f4")  # BIP order
+    (tmp_path / name).write_bytes(cube.tobytes())
+    (tmp_path / (name + ".hdr")).write_text(
+        f"ENVI\nsamples = {W}\nlines = {H}\nbands = {B}\ndata type = 4\ninterleave = bip\nbyte order = 0\n")
+    return str(tmp_path / (name + ".hdr"))
+
+
+def test_envi_source_errors_before_any_device_call(tmp_path):
+    """An ENVI replay without --library stops at the missing library (exit 2), an unreadable
+    header at the reader (exit 1), both before the device is used."""
+    _build()
+    hdr = _envi_cube(tmp_path, "scene", 4, 6, 5, 1)
+    r = _run("--source=envi", f"--envi={hdr}")
+    assert r.returncode == 2 and "no target spectra: pass --library=<csv>" in r.stderr, r.stderr
+    r = _run("--source=envi", f"--envi={tmp_path / 'missing.hdr'}", "--library=/nonexistent.csv")
+    assert r.returncode == 1 and "cannot open spectral library" in r.stderr, r.stderr
+    lib = tmp_path / "lib.csv"
+    lib.write_text("a,0.1,0.2,0.3,0.4,0.5\n")
+    r = _run("--source=envi", f"--envi={tmp_path / 'missing.hdr'}", f"--library={lib}")
+    assert r.returncode == 1 and "cannot open ENVI header" in r.stderr, r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("detector", ["sam", "ace"])
+def test_envi_replay_runs_end_to_end(tmp_path, detector):
+    _build()
+    a = _envi_cube(tmp_path, "a", 64, 96, 24, 2)
+    b = _envi_cube(tmp_path, "b", 64, 96, 24, 3)
+    lib = tmp_path / "lib.csv"
+    lib.write_text("t0," + ",".join(f"{0.2 + 0.01 * i:.3f}" for i in range(24)) + "\n"
+                   + "t1," + ",".join(f"{0.9 - 0.02 * i:.3f}" for i in range(24)) + "\n")
+    r = _run("--source=envi", f"--envi={a},{b}", f"--library={lib}", f"--detector={detector}", "--frames=4",
+             "--warmup=1", timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "envi-replay(2 cubes, 64x96x24)" in r.stdout and "frames 4 in" in r.stdout, r.stdout
