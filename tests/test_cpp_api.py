@@ -26,6 +26,7 @@ REFERENCE_NAMES = [
     "hsi::rx_threshold_for_false_alarm_rate(", "hsi::Pipeline::create(", "hsi::make_synthetic_source(",
     "hsi::moments_from_shifted(", "hsi::SpectralLibrary::flatten(", "hsi::SpectralLibrary::norms(",
     "hsi::convert_interleave(", "hsi::parse_memory_mode(", "hsi::read_spectra_csv(", "hsi::write_spectra_csv(",
+    "hsi::read_envi(", "hsi::parse_envi_header(", "hsi::find_envi_data_file(", "hsi::make_envi_replay_source(",
 ]
 
 
