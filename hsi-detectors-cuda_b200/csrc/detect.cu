@@ -555,14 +555,21 @@ int segs_of(int height, int width) { return height * ((width + kSeg - 1) / kSeg)
 size_t ws_bytes_for_segs(int64_t segs) { return static_cast<size_t>(segs) * sizeof(uint32_t) * (2 + kWordsPerSeg) + 256; }
 
 int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
+  // read once per process (a local static's initialisation is thread-safe)
+  static const int n = [] {
+    int dev = 0, v = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+  }();
   return n;
+}
+
+// Blocks of `kernel` resident per SM at `threads` threads (4 if the query fails).
+template <typename K>
+int resident_blocks(K kernel, int threads) {
+  int v = 0;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, 0) == cudaSuccess && v > 0 ? v : 4;
 }
 
 int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cudaStream_t s) {
@@ -608,17 +615,10 @@ int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cuda
   b.counts = p;
   b.offsets = p + segs;
   b.masks = p + 2 * segs;
-  // one wave of resident tiles per flags kind (41 KB of shared memory each)
-  static int per_sm[2] = {0, 0};
-  if (per_sm[0] == 0) {
-    int v = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, flags_kernel, kFlagThreads, 0) != cudaSuccess || v <= 0) v = 4;
-    per_sm[0] = v;
-    v = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, flags_fast_kernel, kFastThreads, 0) != cudaSuccess || v <= 0)
-      v = 4;
-    per_sm[1] = v;
-  }
+  // one wave of resident tiles per flags kind (41 KB of shared memory each),
+  // the residency read once per process
+  static const int per_sm[2] = {resident_blocks(flags_kernel, kFlagThreads),
+                                resident_blocks(flags_fast_kernel, kFastThreads)};
   const int64_t emit_blocks = (segs + kThreads / 32 - 1) / (kThreads / 32);  // a warp per segment
   const int grid = static_cast<int>(emit_blocks < 16 * sm_count() ? emit_blocks : 16 * sm_count());
   for (int kind = 0; kind < 2; ++kind) {

@@ -585,13 +585,10 @@ int launch_tc(const void* cube, int64_t P, int B, int64_t stride, const double* 
   const int dt = sizeof(T) == 4 ? HSI_F32 : HSI_F16;
   if (encode_cube_map(&map, cube, dt, P, B, stride, kBoxPx, kK) != 0) return HSI_E_INVALID;
   const Smem L = smem_layout<T>();
-  static bool configured[2] = {false, false};
-  if (!configured[sizeof(T) == 4]) {
-    const cudaError_t e = cudaFuncSetAttribute(rxace_tc_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(L.total));
-    if (e != cudaSuccess) return static_cast<int>(e);
-    configured[sizeof(T) == 4] = true;
-  }
+  // set once per process and element type (thread-safe local static)
+  static const cudaError_t configured = cudaFuncSetAttribute(
+      rxace_tc_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.total));
+  if (configured != cudaSuccess) return static_cast<int>(configured);
   TcOperands* ops = static_cast<TcOperands*>(ws);
   const int per_pass = kRows - B < kMaxTargetsPerPass ? kRows - B : kMaxTargetsPerPass;
   const int passes = ntargets > 0 ? (ntargets + per_pass - 1) / per_pass : 1;

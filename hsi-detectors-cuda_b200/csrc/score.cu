@@ -1159,13 +1159,13 @@ __global__ void __launch_bounds__(kHThreads, 1) score_h_kernel(const __grid_cons
 // ---------------------------------------------------------------------------
 
 int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
+  // read once per process (a local static's initialisation is thread-safe)
+  static const int n = [] {
+    int dev = 0, v = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+  }();
   return n;
 }
 
@@ -1183,16 +1183,25 @@ int launch_instance(const ScoreParams& p, int max_bands, int ctas_per_sm, cudaSt
   const SmemLayout L = smem_layout<T>(kGroups, max_bands, score_slots<KS, KC>(), score_stages<T, KS, KC>());
   const int threads = kGroups * kGroupThreads + 32;
   auto kernel = score_kernel<T, KS, KC>;
+  // The attribute and the residency follow the band count of the call; the
+  // lock keeps the pair consistent when host threads launch concurrently.
+  static std::mutex mu;
   static int configured_bytes = -1;
-  static int per_sm = 0;
-  if (configured_bytes != static_cast<int>(L.total)) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(L.total));
-    if (e != cudaSuccess) return static_cast<int>(e);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, L.total);
-    if (e != cudaSuccess) return static_cast<int>(e);
-    if (per_sm < 1) per_sm = 1;
-    configured_bytes = static_cast<int>(L.total);
+  static int configured_per_sm = 0;
+  int per_sm = 0;
+  {
+    const std::lock_guard<std::mutex> lock(mu);
+    if (configured_bytes != static_cast<int>(L.total)) {
+      cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(L.total));
+      if (e != cudaSuccess) return static_cast<int>(e);
+      int v = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, L.total);
+      if (e != cudaSuccess) return static_cast<int>(e);
+      configured_per_sm = v < 1 ? 1 : v;
+      configured_bytes = static_cast<int>(L.total);
+    }
+    per_sm = configured_per_sm;
   }
   // ctas_per_sm: 0 = as many as fit; otherwise that many (capped at what fits)
   const int per = ctas_per_sm > 0 && ctas_per_sm < per_sm ? ctas_per_sm : per_sm;
@@ -1267,14 +1276,11 @@ int launch_h(const HParams& p, cudaStream_t stream) {
   constexpr int N2 = 2 * ((KS + KC + 15) / 16 * 16);
   auto kernel = score_h_kernel<KS, KC>;
   const HSmem L = h_smem(p.bp, N2);
-  static int configured = -1;
-  if (configured < static_cast<int>(L.total)) {
-    const HSmem big = h_smem(kHMaxBands, N2);
-    const cudaError_t e =
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(big.total));
-    if (e != cudaSuccess) return static_cast<int>(e);
-    configured = static_cast<int>(big.total);
-  }
+  // set once per process, at the largest layout (a local static's
+  // initialisation is thread-safe)
+  static const cudaError_t configured = cudaFuncSetAttribute(
+      kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(h_smem(kHMaxBands, N2).total));
+  if (configured != cudaSuccess) return static_cast<int>(configured);
   kernel<<<sm_count(), kHThreads, L.total, stream>>>(p);
   return static_cast<int>(cudaGetLastError());
 }

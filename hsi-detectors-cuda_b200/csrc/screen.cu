@@ -724,13 +724,11 @@ extern "C" HSI_API int hsi_screen_gradients(const float* d_params, int bands, co
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const int Bp = padded_bands(bands);
   const size_t smem = sizeof(float) * (static_cast<size_t>(Bp) * kH1 + kH1 * kH2 + kH2);
-  static bool configured = false;
-  if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(sizeof(float) * (256 * kH1 + kH1 * kH2 + kH2)));
-    if (e != cudaSuccess) return static_cast<int>(e);
-    configured = true;
-  }
+  // set once per process, at the largest band count (thread-safe local static)
+  static const cudaError_t configured = cudaFuncSetAttribute(
+      forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      static_cast<int>(sizeof(float) * (256 * kH1 + kH1 * kH2 + kH2)));
+  if (configured != cudaSuccess) return static_cast<int>(configured);
   const int blocks = (n + kFwdThreads - 1) / kFwdThreads;
   forward_kernel<<<blocks, kFwdThreads, smem, s>>>(d_params, bands, d_features, d_labels, n, pos_weight, t.acts);
   const ParamView g = view(d_grads, bands);

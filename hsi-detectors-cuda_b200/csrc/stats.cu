@@ -1214,13 +1214,13 @@ __global__ void __launch_bounds__(256) quarter_assemble_kernel(const __grid_cons
 // ---------------------------------------------------------------------------
 
 int num_sms() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
+  // read once per process (a local static's initialisation is thread-safe)
+  static const int n = [] {
+    int dev = 0, v = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return v > 0 ? v : 148;
+  }();
   return n;
 }
 
@@ -1355,7 +1355,7 @@ void launch_shift(const FrameTable& t, cudaStream_t s) {
 template <typename T>
 int launch_tensor_group(const hsi_moments_job* const* jobs, int m, void* workspace, cudaStream_t s,
                         int* status, const int* run0 = nullptr, const int64_t* run1_plane = nullptr) {
-  static GemmParams p;  // large (13 KB): kept off the stack; calls are serialised by the caller's thread
+  static thread_local GemmParams p;  // large (13 KB): kept off the stack, one per host thread
   p = GemmParams{};
   FrameTable& t = p.t;
   t.n = m;
@@ -1418,13 +1418,10 @@ int launch_tensor_group(const hsi_moments_job* const* jobs, int m, void* workspa
   }
   if (used > kMaxCtas + m) return HSI_E_CAPACITY;  // cannot happen: pieces <= CTAs + frames - 1
   const StatsSmem L = stats_smem<T>();
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(stats_gemm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(L.total));
-    if (e != cudaSuccess) return static_cast<int>(e);
-    configured = true;
-  }
+  // set once per process and element type (thread-safe local static)
+  static const cudaError_t configured = cudaFuncSetAttribute(
+      stats_gemm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.total));
+  if (configured != cudaSuccess) return static_cast<int>(configured);
   launch_shift<T>(t, s);
   p.conditional = 0;
   stats_gemm_kernel<T><<<grid, kThreads, L.total, s>>>(p);
