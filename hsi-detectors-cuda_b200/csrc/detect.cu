@@ -27,9 +27,12 @@
 // Semantics are the reference CPU path's (src/sam_cpu.cpp:86-138), polarity
 // included; the reference GPU kernel (src/detect.cu:43-87) ignores polarity
 // and emits in atomic arrival order, both of which this replaces.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "common.cuh"
+#include "launch_state.h"
 
 namespace hsi_b200 {
 namespace {
@@ -550,26 +553,24 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(const __grid_constant__ 
   }
 }
 
-int segs_of(int height, int width) { return height * ((width + kSeg - 1) / kSeg); }
+// Row segments of a map; 64-bit, so sizes far past the limits below stay exact.
+int64_t segs_of(int height, int width) {
+  return static_cast<int64_t>(height) * ((static_cast<int64_t>(width) + kSeg - 1) / kSeg);
+}
+
+// Largest segment count of one batch (the kernels index segments in int).
+constexpr int64_t kMaxBatchSegs = 0x3fffffff;
 
 size_t ws_bytes_for_segs(int64_t segs) { return static_cast<size_t>(segs) * sizeof(uint32_t) * (2 + kWordsPerSeg) + 256; }
 
-int sm_count() {
-  // read once per process (a local static's initialisation is thread-safe)
-  static const int n = [] {
-    int dev = 0, v = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
-    return v > 0 ? v : 148;
-  }();
-  return n;
-}
+int sm_count() { return device_sm_count(); }
 
-// Blocks of `kernel` resident per SM at `threads` threads (4 if the query fails).
+// Blocks of `kernel` resident per SM of the current device at `threads`
+// threads (4 if the query fails).
 template <typename K>
-int resident_blocks(K kernel, int threads) {
-  int v = 0;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, 0) == cudaSuccess && v > 0 ? v : 4;
+int resident_blocks(K* kernel, int threads) {
+  const int v = device_residency(kernel, threads, 0);
+  return v > 0 ? v : 4;
 }
 
 int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cudaStream_t s) {
@@ -603,7 +604,7 @@ int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cuda
     b.kind_jobs[kind][b.kind_n[kind]++] = i;
     segs += segs_of(j.height, j.width);
     tiles[kind] += static_cast<int64_t>(J.tiles_x) * ((j.height + kTileH - 1) / kTileH);
-    if (segs > 0x3fffffff || tiles[kind] > 0x3fffffff) return HSI_E_CAPACITY;
+    if (segs > kMaxBatchSegs || tiles[kind] > 0x3fffffff) return HSI_E_CAPACITY;
   }
   if (!ws || ws_bytes < ws_bytes_for_segs(segs)) return HSI_E_WORKSPACE;
   if ((reinterpret_cast<uintptr_t>(ws) & 15u) != 0) return HSI_E_INVALID;
@@ -616,9 +617,9 @@ int run_batch(const hsi_detect_job* jobs, int n, void* ws, size_t ws_bytes, cuda
   b.offsets = p + segs;
   b.masks = p + 2 * segs;
   // one wave of resident tiles per flags kind (41 KB of shared memory each),
-  // the residency read once per process
-  static const int per_sm[2] = {resident_blocks(flags_kernel, kFlagThreads),
-                                resident_blocks(flags_fast_kernel, kFastThreads)};
+  // the residency read once per device
+  const int per_sm[2] = {resident_blocks(flags_kernel, kFlagThreads),
+                         resident_blocks(flags_fast_kernel, kFastThreads)};
   const int64_t emit_blocks = (segs + kThreads / 32 - 1) / (kThreads / 32);  // a warp per segment
   const int grid = static_cast<int>(emit_blocks < 16 * sm_count() ? emit_blocks : 16 * sm_count());
   for (int kind = 0; kind < 2; ++kind) {
@@ -642,7 +643,8 @@ using namespace hsi_b200;
 
 extern "C" HSI_API size_t hsi_detect_workspace_bytes(int height, int width) {
   if (height <= 0 || width <= 0) return 0;
-  return ws_bytes_for_segs(segs_of(height, width));
+  const int64_t segs = segs_of(height, width);
+  return segs > kMaxBatchSegs ? 0 : ws_bytes_for_segs(segs);
 }
 
 extern "C" HSI_API size_t hsi_detect_batch_workspace_bytes(const hsi_detect_job* jobs, int num_jobs) {
@@ -651,6 +653,7 @@ extern "C" HSI_API size_t hsi_detect_batch_workspace_bytes(const hsi_detect_job*
   for (int i = 0; i < num_jobs; ++i) {
     if (jobs[i].height <= 0 || jobs[i].width <= 0) return 0;
     segs += segs_of(jobs[i].height, jobs[i].width);
+    if (segs > kMaxBatchSegs) return 0;
   }
   return ws_bytes_for_segs(segs);
 }
@@ -703,24 +706,70 @@ static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocBytes / size
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mutex;
-void* g_noalloc_addr[kNoAllocMaxDevices];  // device address of the array, per device
+struct NoAllocAddr {
+  unsigned long long context;  // the context the address belongs to (0 = none yet)
+  void* addr;                  // device address of the array in that context
+};
+NoAllocAddr g_noalloc_addr[kNoAllocMaxDevices];
 
-// Once per device, with that device current: look up the array's device
-// address (in host code its name is only a host-side stand-in).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Process-unique id of the current context.  A device reset (or any other
+// re-creation of the context) reloads the module, so the array may move; the
+// id changes with it, where a context handle could be reused.
+int current_context_id(unsigned long long* id) {
+  static const CtxGetCurrentFn get_current = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    return cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess
+               ? reinterpret_cast<CtxGetCurrentFn>(p)
+               : nullptr;
+  }();
+  static const CtxGetIdFn get_id = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    return cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess
+               ? reinterpret_cast<CtxGetIdFn>(p)
+               : nullptr;
+  }();
+  if (!get_current || !get_id) return HSI_E_NO_DEVICE;
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return HSI_E_NO_DEVICE;
+  return get_id(ctx, id) == CUDA_SUCCESS ? HSI_OK : HSI_E_NO_DEVICE;
+}
+
+// Once per device (and again whenever that device's context is re-created),
+// with the device current: look up the array's device address (in host code
+// its name is only a host-side stand-in).
 int noalloc_scratch(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return static_cast<int>(e);
   if (dev < 0 || dev >= kNoAllocMaxDevices) return HSI_E_NO_DEVICE;
+  unsigned long long ctx = 0;
+  if (current_context_id(&ctx) != HSI_OK) {
+    // no context is current before the runtime's first call on this thread:
+    // the symbol lookup makes the device's primary context current
+    void* addr = nullptr;
+    e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess) return static_cast<int>(e);
+    const int st = current_context_id(&ctx);
+    if (st != HSI_OK) return st;
+  }
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (g_noalloc_addr[dev] == nullptr) {
+  NoAllocAddr& a = g_noalloc_addr[dev];
+  if (a.addr == nullptr || a.context != ctx) {
     void* addr = nullptr;
     e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
     if (e != cudaSuccess) return static_cast<int>(e);
     if ((reinterpret_cast<uintptr_t>(addr) & 255u) != 0) return HSI_E_INVALID;
-    g_noalloc_addr[dev] = addr;
+    a.addr = addr;
+    a.context = ctx;
   }
-  *out = g_noalloc_addr[dev];
+  *out = a.addr;
   return HSI_OK;
 }
 

@@ -6,6 +6,7 @@
 #include <cuda_fp16.h>
 
 #include "common.cuh"
+#include "launch_state.h"
 #include "synth.h"
 
 namespace hsi_b200 {
@@ -97,13 +98,13 @@ extern "C" HSI_API int hsi_generate(const hsi_scene* scene, const float* d_spect
   if (blocks > 148 * 16) blocks = 148 * 16;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (dtype == HSI_F32) {
-    cudaFuncSetAttribute(generate_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(smem));
+    const cudaError_t e = raise_smem_limit(generate_kernel<float>, static_cast<int>(smem));
+    if (e != cudaSuccess) return static_cast<int>(e);
     generate_kernel<float><<<blocks, 256, smem, s>>>(spec, d_spectra, pixels, pixel0,
                                                      static_cast<float*>(d_cube), plane_stride, d_truth);
   } else if (dtype == HSI_F16) {
-    cudaFuncSetAttribute(generate_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(smem));
+    const cudaError_t e = raise_smem_limit(generate_kernel<__half>, static_cast<int>(smem));
+    if (e != cudaSuccess) return static_cast<int>(e);
     generate_kernel<__half><<<blocks, 256, smem, s>>>(spec, d_spectra, pixels, pixel0,
                                                       static_cast<__half*>(d_cube), plane_stride, d_truth);
   } else {

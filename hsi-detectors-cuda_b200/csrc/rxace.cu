@@ -18,6 +18,7 @@
 // all-zero upper-triangle K-chunks of W): the comparator for the tensor-core
 // path in whiten.cu.
 #include "common.cuh"
+#include "launch_state.h"
 
 namespace hsi_b200 {
 namespace {
@@ -303,11 +304,13 @@ extern "C" HSI_API int hsi_rx_ace_simt(const void* d_cube, int height, int width
   const unsigned blocks = static_cast<unsigned>(div_up<int64_t>(P, kPxTile));
   const int smem = static_cast<int>(sizeof(SimtSmem));
   if (dtype == HSI_F32) {
-    cudaFuncSetAttribute(rxace_simt_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const cudaError_t e = raise_smem_limit(rxace_simt_kernel<float>, smem);
+    if (e != cudaSuccess) return static_cast<int>(e);
     rxace_simt_kernel<float><<<blocks, kThreads, smem, s>>>(static_cast<const float*>(d_cube), P, plane_stride,
                                                             bands, num_targets, op, o);
   } else {
-    cudaFuncSetAttribute(rxace_simt_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const cudaError_t e = raise_smem_limit(rxace_simt_kernel<__half>, smem);
+    if (e != cudaSuccess) return static_cast<int>(e);
     rxace_simt_kernel<__half><<<blocks, kThreads, smem, s>>>(static_cast<const __half*>(d_cube), P, plane_stride,
                                                              bands, num_targets, op, o);
   }

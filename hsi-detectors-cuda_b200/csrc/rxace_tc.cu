@@ -41,6 +41,7 @@
 #include <type_traits>
 
 #include "tc.cuh"
+#include "launch_state.h"
 
 namespace hsi_b200 {
 namespace {
@@ -571,12 +572,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 size_t tc_ws_bytes() { return (sizeof(TcOperands) + 255) & ~size_t(255); }
 
-int sm_count() {
-  int dev = 0, n = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-  return n > 0 ? n : 148;
-}
+int sm_count() { return device_sm_count(); }
 
 template <typename T>
 int launch_tc(const void* cube, int64_t P, int B, int64_t stride, const double* stats, int ntargets, float* rx,
@@ -585,9 +581,8 @@ int launch_tc(const void* cube, int64_t P, int B, int64_t stride, const double* 
   const int dt = sizeof(T) == 4 ? HSI_F32 : HSI_F16;
   if (encode_cube_map(&map, cube, dt, P, B, stride, kBoxPx, kK) != 0) return HSI_E_INVALID;
   const Smem L = smem_layout<T>();
-  // set once per process and element type (thread-safe local static)
-  static const cudaError_t configured = cudaFuncSetAttribute(
-      rxace_tc_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.total));
+  // set once per device and element type
+  const cudaError_t configured = raise_smem_limit(rxace_tc_kernel<T>, static_cast<int>(L.total));
   if (configured != cudaSuccess) return static_cast<int>(configured);
   TcOperands* ops = static_cast<TcOperands*>(ws);
   const int per_pass = kRows - B < kMaxTargetsPerPass ? kRows - B : kMaxTargetsPerPass;

@@ -23,6 +23,7 @@
 #include <cuda_fp16.h>
 
 #include "synth.h"
+#include "launch_state.h"
 #include "tc.cuh"
 
 namespace hsi_b200 {
@@ -724,10 +725,9 @@ extern "C" HSI_API int hsi_screen_gradients(const float* d_params, int bands, co
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const int Bp = padded_bands(bands);
   const size_t smem = sizeof(float) * (static_cast<size_t>(Bp) * kH1 + kH1 * kH2 + kH2);
-  // set once per process, at the largest band count (thread-safe local static)
-  static const cudaError_t configured = cudaFuncSetAttribute(
-      forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-      static_cast<int>(sizeof(float) * (256 * kH1 + kH1 * kH2 + kH2)));
+  // the largest band count's layout, set once per device
+  const cudaError_t configured =
+      raise_smem_limit(forward_kernel, static_cast<int>(sizeof(float) * (256 * kH1 + kH1 * kH2 + kH2)));
   if (configured != cudaSuccess) return static_cast<int>(configured);
   const int blocks = (n + kFwdThreads - 1) / kFwdThreads;
   forward_kernel<<<blocks, kFwdThreads, smem, s>>>(d_params, bands, d_features, d_labels, n, pos_weight, t.acts);
@@ -779,13 +779,9 @@ extern "C" HSI_API int hsi_screen_infer(const void* d_cube, int height, int widt
   CUtensorMap map;
   if (encode_cube_map_sw128(&map, d_cube, HSI_F16, P, bands, plane_stride, kScrBox, Bp) != 0) return HSI_E_INVALID;
   const size_t smem = screen_smem_bytes(Bp);
-  const cudaError_t e = cudaFuncSetAttribute(screen_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem));
+  const cudaError_t e = raise_smem_limit(screen_tc_kernel, static_cast<int>(smem));
   if (e != cudaSuccess) return static_cast<int>(e);
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (sms <= 0) sms = 148;
+  const int sms = device_sm_count();
   const int64_t ntiles = (P + kScrTile - 1) / kScrTile;
   const int grid = static_cast<int>(ntiles < sms ? ntiles : sms);
   ScreenArgs a{P, Bp, ops, d_logits, nullptr};

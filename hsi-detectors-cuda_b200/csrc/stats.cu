@@ -58,9 +58,11 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "tc.cuh"
+#include "launch_state.h"
 
 namespace hsi_b200 {
 namespace {
@@ -1213,16 +1215,7 @@ __global__ void __launch_bounds__(256) quarter_assemble_kernel(const __grid_cons
 // Host side
 // ---------------------------------------------------------------------------
 
-int num_sms() {
-  // read once per process (a local static's initialisation is thread-safe)
-  static const int n = [] {
-    int dev = 0, v = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
-    return v > 0 ? v : 148;
-  }();
-  return n;
-}
+int num_sms() { return device_sm_count(); }
 
 constexpr int kSimtSlices = 96;
 
@@ -1316,16 +1309,24 @@ using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+EncodeTiledFn lookup_encode_fn() {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+      q == cudaDriverEntryPointSuccess)
+    return reinterpret_cast<EncodeTiledFn>(p);
+  return nullptr;
+}
+
+// The driver's entry point is process-wide; a failed lookup is retried.
 EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
+  static std::atomic<EncodeTiledFn> fn{nullptr};
+  EncodeTiledFn f = fn.load(std::memory_order_acquire);
+  if (!f) {
+    f = lookup_encode_fn();
+    if (f) fn.store(f, std::memory_order_release);
   }
-  return fn;
+  return f;
 }
 
 FrameStats frame_of_job(const hsi_moments_job& j) {
@@ -1418,9 +1419,8 @@ int launch_tensor_group(const hsi_moments_job* const* jobs, int m, void* workspa
   }
   if (used > kMaxCtas + m) return HSI_E_CAPACITY;  // cannot happen: pieces <= CTAs + frames - 1
   const StatsSmem L = stats_smem<T>();
-  // set once per process and element type (thread-safe local static)
-  static const cudaError_t configured = cudaFuncSetAttribute(
-      stats_gemm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.total));
+  // set once per device and element type
+  const cudaError_t configured = raise_smem_limit(stats_gemm_kernel<T>, static_cast<int>(L.total));
   if (configured != cudaSuccess) return static_cast<int>(configured);
   launch_shift<T>(t, s);
   p.conditional = 0;
@@ -1445,7 +1445,7 @@ int launch_simt_stats(const hsi_moments_job& j, void* workspace, cudaStream_t s)
   double* partials = reinterpret_cast<double*>(w + align256(sizeof(StatsState)));
   double* fsum = reinterpret_cast<double*>(w + align256(sizeof(StatsState)) +
                                            align256(static_cast<size_t>(kSimtSlices) * n * n * sizeof(double)));
-  static FrameTable t;  // 5.7 KB: kept off the stack
+  static thread_local FrameTable t;  // 5.7 KB: kept off the stack, one per host thread
   t = FrameTable{};
   t.n = 1;
   t.max_bands = B;

@@ -436,8 +436,10 @@ HSI_API int hsi_accumulate_shifted_moments(const double* d_moments, const float*
  *  - the scratch needs no clearing; as with hsi_detect, *d_count is the
  *    append offset the caller sets (normally zero) before the call;
  *  - the first call on each device does a one-time set-up (it looks up the
- *    array's device address and sets the detection kernel's shared-memory
- *    limit), so that first call should come before any stream capture.
+ *    array's device address in the current context and reads the detection
+ *    kernels' residency), so that first call should come before any stream
+ *    capture; the set-up runs again after the device's context is re-created
+ *    (for example by cudaDeviceReset), since the array may then move.
  * It calls no allocating routine.  HSI_E_NO_DEVICE for device ordinals >= 64. */
 #define HSI_DETECT_NOALLOC_MAX_SEGMENTS 8192
 HSI_API int hsi_detect_noalloc(const float* d_score, const int32_t* d_target, int height, int width,
