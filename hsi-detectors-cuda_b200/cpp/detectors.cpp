@@ -8,6 +8,7 @@
 
 #include "hsi/sam_cuda.hpp"
 #include "status.hpp"
+#include "workspace.hpp"
 
 namespace hsi {
 
@@ -104,16 +105,17 @@ cudaError_t launch_rx_ace(const void* d_cube, CubeShape shape, bool half, const 
                           std::size_t map_stride, cudaStream_t stream) {
   if (!d_cube || !shape.valid() || shape.bands != stats.bands() || !stats.packed()) return cudaErrorInvalidValue;
   const int T = (d_ace_best || d_ace_target || d_ace_maps) ? stats.num_targets() : 0;
-  const std::size_t ws = hsi_rx_ace_simt_workspace_bytes(shape.bands, T);
+  // the tensor-core whitening holds up to 127 bands; wider cubes take the FP32 CUDA-core kernel
+  const bool tensor = shape.bands <= 127;
+  const std::size_t ws = tensor ? hsi_rx_ace_workspace_bytes(shape.bands, T)
+                                : hsi_rx_ace_simt_workspace_bytes(shape.bands, T);
   void* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(&scratch, ws, stream);
+  const cudaError_t e = detail::stream_scratch(stream, ws, &scratch);
   if (e != cudaSuccess) return e;
-  const int st = hsi_rx_ace_simt(d_cube, shape.height, shape.width, shape.bands, half ? HSI_F16 : HSI_F32,
-                                 static_cast<int64_t>(bsq_plane_stride(shape)), stats.packed(), T, d_rx, d_ace_best,
-                                 d_ace_target, d_ace_maps, static_cast<int64_t>(map_stride), scratch, ws,
-                                 as_stream(stream));
-  e = cudaFreeAsync(scratch, stream);
-  return st != HSI_OK ? to_cuda(st) : e;
+  const auto fn = tensor ? hsi_rx_ace : hsi_rx_ace_simt;
+  return to_cuda(fn(d_cube, shape.height, shape.width, shape.bands, half ? HSI_F16 : HSI_F32,
+                    static_cast<int64_t>(bsq_plane_stride(shape)), stats.packed(), T, d_rx, d_ace_best, d_ace_target,
+                    d_ace_maps, static_cast<int64_t>(map_stride), scratch, ws, as_stream(stream)));
 }
 
 cudaError_t launch_cem(const void* d_cube, CubeShape shape, bool half, const DeviceStatistics& stats, float* d_best,

@@ -5,6 +5,7 @@
 
 #include "hsi/detect_cuda.hpp"
 #include "status.hpp"
+#include "workspace.hpp"
 
 namespace hsi {
 
@@ -83,15 +84,12 @@ cudaError_t launch_sam_best(SamVariant variant, const void* d_cube, CubeShape sh
   if (variant == SamVariant::Half) {
     dtype = HSI_F16;
   } else if (variant == SamVariant::BipDirect) {
-    const cudaError_t e = cudaMallocAsync(&scratch, stride * shape.bands * sizeof(float), stream);
+    const cudaError_t e = detail::stream_scratch(stream, stride * shape.bands * sizeof(float), &scratch);
     if (e != cudaSuccess) return e;
     const int st = hsi_transpose_bip_to_bsq(static_cast<const float*>(d_cube), static_cast<float*>(scratch),
                                             shape.height, shape.width, shape.bands,
                                             static_cast<int64_t>(stride), as_stream(stream));
-    if (st != HSI_OK) {
-      cudaFreeAsync(scratch, stream);
-      return to_cuda(st);
-    }
+    if (st != HSI_OK) return to_cuda(st);
     cube = scratch;
   }
   hsi_frame f = frame_of(cube, shape, dtype, stride);
@@ -100,9 +98,7 @@ cudaError_t launch_sam_best(SamVariant variant, const void* d_cube, CubeShape sh
   f.num_sam = num_targets;
   f.sam_best = d_score;
   f.sam_best_target = d_target_id;
-  const int st = hsi_score_frames(&f, 1, as_stream(stream));
-  if (scratch) cudaFreeAsync(scratch, stream);
-  return to_cuda(st);
+  return to_cuda(hsi_score_frames(&f, 1, as_stream(stream)));
 }
 
 cudaError_t launch_sam_maps(const void* d_cube, CubeShape shape, bool half, const float* d_targets,
@@ -137,16 +133,16 @@ cudaError_t launch_detect(const float* d_score, const std::int32_t* d_target_id,
       (params.max_detections > 0 && !d_out))
     return cudaErrorInvalidValue;
   const std::size_t bytes = hsi_detect_workspace_bytes(shape.height, shape.width);
+  if (bytes == 0) return cudaErrorInvalidValue;  // beyond the detection kernels' segment limit
   void* ws = nullptr;
-  cudaError_t e = cudaMallocAsync(&ws, bytes, stream);
+  const cudaError_t e = detail::stream_scratch(stream, bytes, &ws);
   if (e != cudaSuccess) return e;
   const int st = hsi_detect(d_score, d_target_id, shape.height, shape.width, params.threshold, params.nms_radius,
                             params.polarity == ScorePolarity::HigherIsBetter ? HSI_HIGHER_IS_BETTER
                                                                              : HSI_LOWER_IS_BETTER,
                             params.max_detections, reinterpret_cast<hsi_detection*>(d_out), d_count, ws, bytes,
                             as_stream(stream));
-  e = cudaFreeAsync(ws, stream);
-  return st != HSI_OK ? to_cuda(st) : e;
+  return to_cuda(st);
 }
 
 }  // namespace hsi

@@ -9,6 +9,7 @@
 #include "hsi/detector.hpp"
 #include "hsi/sam_cuda.hpp"
 #include "status.hpp"
+#include "workspace.hpp"
 
 namespace hsi {
 
@@ -34,7 +35,8 @@ cudaError_t accumulate(const float* d_cube, CubeShape shape, const float* d_refe
   const std::size_t m_bytes = sizeof(double) * (B + moment_outer_elements(B) + 1);
   const std::size_t o_bytes = d_outer ? 0 : sizeof(double) * moment_outer_elements(B);
   char* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), ws_bytes + m_bytes + o_bytes, stream);
+  const cudaError_t e =
+      detail::stream_scratch(stream, ws_bytes + m_bytes + o_bytes, reinterpret_cast<void**>(&scratch));
   if (e != cudaSuccess) return e;
   double* moments = reinterpret_cast<double*>(scratch + ws_bytes);
   double* outer = d_outer ? d_outer : reinterpret_cast<double*>(scratch + ws_bytes + m_bytes);
@@ -42,8 +44,7 @@ cudaError_t accumulate(const float* d_cube, CubeShape shape, const float* d_refe
                              static_cast<int64_t>(bsq_plane_stride(shape)), moments, d_reference, scratch, ws_bytes,
                              as_stream(stream));
   if (st == HSI_OK) st = hsi_accumulate_shifted_moments(moments, d_reference, B, d_sum, outer, as_stream(stream));
-  e = cudaFreeAsync(scratch, stream);
-  return st != HSI_OK ? to_cuda(st) : e;
+  return to_cuda(st);
 }
 
 }  // namespace

@@ -15,7 +15,9 @@
 
 namespace hsi {
 
-// Scratch is stream-ordered (cudaMallocAsync / cudaFreeAsync on `stream`).
+// Scratch is the stream's grow-only launch workspace (release_launch_workspaces
+// in hsi/sam_cuda.hpp): after the first call at the largest map size on a
+// stream, calls allocate nothing.
 cudaError_t launch_detect(const float* d_score, const std::int32_t* d_target_id, CubeShape shape,
                           DetectionParams params, Detection* d_out, unsigned int* d_count, cudaStream_t stream);
 
