@@ -80,6 +80,9 @@ def parse():
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the extra records of the default run (RX/ACE, screen, same-shape SAM scorer, "
+                         "the reference's GPU SAM comparator)")
     return ap.parse_args()
 
 
@@ -148,6 +151,48 @@ def cpu_reference(workload, sample_rows, repeats, threads=None):
     return times, threads, P
 
 
+# Shapes of the same-box GPU comparison of SAM scorers: the plain-SAM
+# configuration (one target) and the SAM+CEM video frame (eight targets).
+SAM_SHAPES = [(520, 696, 113, 1), (1024, 1024, 113, 8)]
+BENCH_SAM = os.path.join(REPO, "oracle", "_ref", "bench_sam")
+
+
+def reference_gpu_sam(timeout=300):
+    """The reference's own GPU SAM kernels on this GPU: its unmodified
+    bench/bench_sam.cu, built for sm_100a by oracle/Makefile, run at each of
+    SAM_SHAPES.  Returns {shape: {variant: {"ms", "mpix_s"}}} from its
+    throughput table (median of its timed passes, one resident cube), or a
+    reason string."""
+    if not os.path.exists(BENCH_SAM):
+        return "oracle/_ref/bench_sam is not built"
+    out = {}
+    for h, w, b, t in SAM_SHAPES:
+        cmd = [BENCH_SAM, f"--height={h}", f"--width={w}", f"--bands={b}", f"--targets={t}",
+               "--iterations=50", "--warmup-ms=500", "--repeats=5"]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+        rows, table, verdicts = {}, False, {}
+        for line in r.stdout.splitlines():
+            parts = line.split()
+            if "Gpix/s" in line and parts and parts[0] == "variant":
+                table = True
+                continue
+            if parts and parts[0] in ("baseline", "optimized", "half", "bip"):
+                if table and len(parts) >= 8:
+                    ms = float(parts[1])
+                    rows[parts[0]] = {"ms": ms, "mpix_s": round(h * w / (ms / 1e3) / 1e6, 1)}
+                elif not table and ("PASS" in parts or "FAIL" in parts):
+                    verdicts[parts[0]] = "PASS" if "PASS" in parts else "FAIL"
+            if line.startswith("optimized, pixels per thread"):
+                table = False
+        if r.returncode != 0 and not rows:
+            return f"bench_sam exited {r.returncode}: {r.stderr.strip()[-200:]}"
+        for k, v in verdicts.items():
+            if k in rows:
+                rows[k]["check_vs_cpu"] = v
+        out[f"{h}x{w}x{b}, {t} target(s)"] = rows
+    return out
+
+
 def run_reference(args, workload):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -157,16 +202,31 @@ def run_reference(args, workload):
     timed = times[args.warmup:]
     t = float(np.mean(timed))
     value = threads * P / t / 1e6
+    gpu_cmp = None
+    if not args.no_extras:
+        try:
+            gpu_cmp = reference_gpu_sam()
+        except Exception as e:  # the comparator is extra information; the CPU arm stands without it
+            gpu_cmp = f"{type(e).__name__}: {e}"
+    config = workload_config(workload, args.frames, reference=True)
+    config["deviation"] = (f"the CPU arm times {threads} sample frames of {W}x{rows}x{B} per step (one per host "
+                           f"thread) and reports Mpix/s; the GPU arm's frames are {H}x{W}x{B}")
     line = {
         "impl": "reference", "metric": metric_name(workload), "value": round(value, 3), "unit": "Mpix/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded scene model, host-generated)",
-        "config": workload_config(workload, args.frames, reference=True),
+        "config": config,
         "cpu_baseline": {"value": round(value, 3), "unit": "Mpix/s", "cores": threads, "kind": "reference",
                          "sample": f"{threads} frames of {W}x{rows}x{B} per step, one per thread"},
         "e2e": {"value": round(value, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if gpu_cmp is not None:
+        line["gpu_comparator"] = {
+            "what": "the reference's own GPU SAM kernels (src/sam.cu via its bench/bench_sam.cu, unmodified, "
+                    "built for sm_100a) on this GPU: best angle + id, one resident cube, median of 5 passes of "
+                    "50 launches; its own synthetic source",
+            "results": gpu_cmp}
     print(json.dumps(line), flush=True)
 
 
@@ -556,9 +616,81 @@ def run_ours(args, workload):
         }
         if f16 is not None:
             line["f16_variant"] = f16
+        if world == 1 and not args.no_extras:
+            extra_records(args, device, line)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def same_shape_scorer(hsi, torch, device, passes=5, iterations=50, warm_s=0.5):
+    """This library's SAM scorer (best angle + id, no per-target maps) at the
+    shapes the reference's bench_sam is run at (SAM_SHAPES), timed the way
+    bench_sam times its kernels: one resident cube, CUDA events around
+    `iterations` launches, the median of `passes` passes, after a warm-up in
+    wall time.  FP32 and FP16 cubes."""
+    out = {}
+    stream = torch.cuda.current_stream(device)
+    for h, w, b, t in SAM_SHAPES:
+        P = h * w
+        rec = {}
+        sc = hsi.scene(b, n_targets=t, target_frac=0.005 if t == 1 else 0.002, library_seed=0x5EED0000)
+        targets = hsi.scene_targets(sc)
+        tg = torch.from_numpy(targets).to(device)
+        nr = torch.from_numpy(hsi.target_norms(targets)).to(device)
+        best = torch.empty(P, device=device)
+        bt = torch.empty(P, dtype=torch.int32, device=device)
+        for dt, name, esize in ((hsi.F32, "f32", 4), (hsi.F16, "f16", 2)):
+            cube, _ = hsi.generate(sc, h, w, dtype=dt, truth=False, device=device)
+            frames = [hsi.make_frame(cube, h, w, b, dt, sam_targets=tg, sam_norms=nr, sam_best=best,
+                                     sam_best_target=bt, map_stride=P)]
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < warm_s:
+                for _ in range(16):
+                    hsi.score_frames_batch(frames, stream=stream)
+                torch.cuda.synchronize()
+            samples = []
+            for _ in range(passes):
+                a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                for _ in range(iterations):
+                    hsi.score_frames_batch(frames, stream=stream)
+                e.record(stream)
+                torch.cuda.synchronize()
+                samples.append(a.elapsed_time(e) / iterations)
+            ms = float(np.median(samples))
+            rec[name] = {"ms": round(ms, 4), "mpix_s": round(P / (ms / 1e3) / 1e6, 1),
+                         "gb_s": round(P * (esize * b + 8) / (ms / 1e3) / 1e9, 1)}
+            del cube
+        out[f"{h}x{w}x{b}, {t} target(s)"] = rec
+        del best, bt
+    torch.cuda.empty_cache()
+    return {"what": "hsi_score_frames_batch (score_kernel for f32, score_h_kernel for f16): best angle + id, "
+                    "one resident cube, median of 5 passes of 50 launches, as the reference's bench_sam times its "
+                    "kernels (its figures: the reference arm's gpu_comparator)",
+            "results": out}
+
+
+def extra_records(args, device, line):
+    """The default run's other records, each measured after the headline
+    (single GPU only): the RX+ACE precision workload, the learned screen, and
+    the SAM scorer at the shapes of the reference's GPU comparator."""
+    import torch
+    import hsi_b200 as hsi
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup, sub.no_e2e = min(max(args.steps, 3), 10), 3, True
+    for key, fn in (("rx_ace", measure_rxace), ("screen", measure_screen)):
+        try:
+            rec = fn(sub, None, 1, 0, device)
+            rec.pop("e2e", None)
+            line[key] = rec
+        except Exception as e:  # reported, never hidden
+            line[key] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+    try:
+        line["same_shape_scorer"] = same_shape_scorer(hsi, torch, device)
+    except Exception as e:
+        line["same_shape_scorer"] = {"error": f"{type(e).__name__}: {e}"}
 
 
 # DRAM bytes (read + write) per frame of the scoring kernel, from the ncu
@@ -673,11 +805,9 @@ def _fp64_reference(torch, cube, H, Wd, lib, rows):
     return rx, maps
 
 
-def run_rxace(args):
-    import ctypes as C
+def init_ranks(timeout_s=300):
+    """(torch, dist or None, world, rank, device) for a one-process-per-GPU run."""
     import torch
-    import hsi_b200 as hsi
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -685,9 +815,28 @@ def run_rxace(args):
     if world > 1:
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=timeout_s))
     device = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(device)
+    return torch, dist, world, rank, device
+
+
+def run_rxace(args):
+    torch, dist, world, rank, device = init_ranks()
+    line = measure_rxace(args, dist, world, rank, device)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def measure_rxace(args, dist, world, rank, device):
+    """The RX+ACE precision workload; returns its JSON record."""
+    import ctypes as C
+    import torch
+    import hsi_b200 as hsi
+
     L = hsi.lib()
     H, Wd, T = RX_H, RX_W, TARGETS
     P = H * Wd
@@ -752,18 +901,19 @@ def run_rxace(args):
     plain_ms, plain_kern = timed(True, max(2, args.steps // 2), 1)
     ms, kern_ms, plain_ms, plain_kern = max_over_ranks(dist, [ms, kern_ms, plain_ms, plain_kern], device)
 
-    # error of the measured path against a torch FP64 reference (first 64 rows)
+    # error of the measured path against a torch FP64 reference on every pixel
     statistics(cube)
     score(cube, False)
     torch.cuda.synchronize()
-    rows = 64
+    rows = H
     rx64, maps64 = _fp64_reference(torch, cube, H, Wd, lib, rows)
     n = rows * Wd
     rx_err = ((rx[:n].double() - rx64).abs() / rx64.abs().clamp(min=1.0))
     map_err = (maps[:, :n].double() - maps64).abs()
     best64 = maps64.clamp(0, 1).max(dim=0).values
     ace_err = (ab[:n].double() - best64).abs()
-    errors = {"reference": "torch FP64 statistics of the whole frame + FP64 scores, first 64 rows (65536 px)",
+    del rx64, maps64, best64
+    errors = {"reference": f"torch FP64 statistics and FP64 scores of the whole frame ({n} px, every pixel)",
               "rx_rel": {"max": float(rx_err.max()), "mean": float(rx_err.mean())},
               "ace_best_abs": {"max": float(ace_err.max()), "mean": float(ace_err.mean())},
               "ace_maps_abs": {"max": [float(v) for v in map_err.max(dim=1).values],
@@ -825,14 +975,16 @@ def run_rxace(args):
                          "traffic": load_traffic("rx_ace", 1),
                          "kernel_ms": round(kern_ms, 3), "algorithmic_bytes_per_launch": P * per_px},
             "plain_fp32": {"step_ms": round(plain_ms, 3), "kernel_ms": round(plain_kern, 3),
+                           "step_mpix_s": round(world * P / (plain_ms / 1e3) / 1e6, 2),
                            "kernel_mpix_s": round(P / (plain_kern / 1e3) / 1e6, 1),
-                           "tensor_core_speedup": round(plain_kern / kern_ms, 2)},
+                           "tensor_core_speedup": round(plain_kern / kern_ms, 2),
+                           "step_speedup": round(plain_ms / ms, 2)},
             "errors_vs_fp64": errors,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 6 + 1 + 2, "clocks": clocks.summary(),
         }
-        print(json.dumps(line), flush=True)
-    if dist:
-        dist.destroy_process_group()
+    del rx, ab, at, maps, sws, tws, pws
+    torch.cuda.empty_cache()
+    return line if rank == 0 else None
 
 
 # ---------------------------------------------------------------------------
@@ -848,20 +1000,21 @@ SCR_CAP = 1 << 18      # compact re-score capacity; beyond it the plain detector
 
 
 def run_screen(args):
+    torch, dist, world, rank, device = init_ranks(600)
+    line = measure_screen(args, dist, world, rank, device)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def measure_screen(args, dist, world, rank, device):
+    """The learned-screen workload (training, then inference against plain ACE);
+    returns its JSON record."""
     import ctypes as C
     import torch
     import hsi_b200 as hsi
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
-    device = torch.device("cuda", local if world > 1 else 0)
-    torch.cuda.set_device(device)
     L = hsi.lib()
     Bs, T = SCR_B, SCR_T
     lib_seed = 0x5EED5000
@@ -1057,9 +1210,9 @@ def run_screen(args):
             "train_seconds": round(train_s, 2),
             "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": clocks.summary(),
         }
-        print(json.dumps(line), flush=True)
-    if dist:
-        dist.destroy_process_group()
+    del cube, logits, ace_full, compact, screen
+    torch.cuda.empty_cache()
+    return line if rank == 0 else None
 
 
 # ---------------------------------------------------------------------------
