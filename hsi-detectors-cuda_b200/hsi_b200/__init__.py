@@ -606,6 +606,27 @@ class BatchTuning(C.Structure):
                 ("plain_rx_frames", C.c_int32), ("tuning_ms", C.c_float)]
 
 
+LAGGED_SAM_CEM = 1
+LAGGED_RX_ACE = 2
+
+
+class LaggedOptions(C.Structure):
+    _fields_ = [("height", C.c_int32), ("width", C.c_int32), ("bands", C.c_int32), ("dtype", C.c_int32),
+                ("targets", C.c_void_p), ("num_targets", C.c_int32), ("detectors", C.c_int32),
+                ("loading", C.c_double), ("sam_threshold", C.c_float), ("cem_threshold", C.c_float),
+                ("ace_threshold", C.c_float), ("rx_false_alarm_rate", C.c_double), ("nms_radius", C.c_int32),
+                ("capacity", C.c_int32)]
+
+
+class LaggedOutputs(C.Structure):
+    _fields_ = [("frame", C.c_int64), ("statistics_frame", C.c_int64), ("sam_maps", C.c_void_p),
+                ("sam_best", C.c_void_p), ("sam_target", C.c_void_p), ("cem_maps", C.c_void_p),
+                ("cem_best", C.c_void_p), ("cem_target", C.c_void_p), ("rx", C.c_void_p), ("ace_maps", C.c_void_p),
+                ("ace_best", C.c_void_p), ("ace_target", C.c_void_p), ("detections", C.c_void_p * 4),
+                ("counts", C.c_void_p), ("status", C.c_void_p), ("map_stride", C.c_int64),
+                ("rx_threshold", C.c_float)]
+
+
 def cxx_lib():
     """libhsi_cxx.so (C++ API and the batch runner's C ABI); raises if not built."""
     global _cxx
@@ -626,6 +647,14 @@ def cxx_lib():
         L.hsi_batch_tuning_of.restype = i32
         L.hsi_batch_destroy.argtypes = [vp]
         L.hsi_batch_destroy.restype = None
+        L.hsi_lagged_create.argtypes = [C.POINTER(LaggedOptions), C.POINTER(C.c_int)]
+        L.hsi_lagged_create.restype = vp
+        L.hsi_lagged_push.argtypes = [vp, vp, vp]
+        L.hsi_lagged_push.restype = i32
+        L.hsi_lagged_outputs_of.argtypes = [vp, C.POINTER(LaggedOutputs)]
+        L.hsi_lagged_outputs_of.restype = i32
+        L.hsi_lagged_destroy.argtypes = [vp]
+        L.hsi_lagged_destroy.restype = None
         _cxx = L
     return _cxx
 
@@ -682,6 +711,44 @@ class Batch:
     def close(self):
         if self.handle:
             cxx_lib().hsi_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Lagged:
+    """The lagged-statistics video runner (include/hsi_lagged.h): push device
+    cubes of one shape in order; frame k is scored with frame k-1's statistics
+    while frame k's own are built on an internal stream."""
+
+    def __init__(self, height, width, bands, targets, dtype=F32, detectors=LAGGED_SAM_CEM | LAGGED_RX_ACE,
+                 loading=1e-6, sam_threshold=0.10, cem_threshold=0.5, ace_threshold=0.5, rx_false_alarm_rate=1e-3,
+                 nms_radius=2, capacity=4096):
+        import numpy as np
+        L = cxx_lib()
+        self._tg = np.ascontiguousarray(targets, np.float32)
+        opt = LaggedOptions(height, width, bands, dtype, self._tg.ctypes.data, self._tg.shape[0], detectors, loading,
+                            sam_threshold, cem_threshold, ace_threshold, rx_false_alarm_rate, nms_radius, capacity)
+        st = C.c_int(0)
+        self.handle = L.hsi_lagged_create(C.byref(opt), C.byref(st))
+        check(st.value, "hsi_lagged_create")
+        self.height, self.width, self.bands, self.targets, self.capacity = height, width, bands, self._tg.shape[0], capacity
+
+    def push(self, cube, stream=None):
+        check(cxx_lib().hsi_lagged_push(self.handle, _ptr(cube), _stream(stream)), "hsi_lagged_push")
+
+    def outputs(self):
+        o = LaggedOutputs()
+        check(cxx_lib().hsi_lagged_outputs_of(self.handle, C.byref(o)), "hsi_lagged_outputs_of")
+        return o
+
+    def close(self):
+        if self.handle:
+            cxx_lib().hsi_lagged_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -1,6 +1,7 @@
 """The C-ABI libraries load and export every entry point include/*.h declares:
-include/hsi_b200.h from libhsi_b200.so (kernels), include/hsi_batch.h from
-libhsi_cxx.so (the batch runner, host C++ over the first).
+include/hsi_b200.h from libhsi_b200.so (kernels), include/hsi_batch.h and
+include/hsi_lagged.h from libhsi_cxx.so (the batch and lagged-statistics
+runners, host C++ over the first).
 
 No compute calls: these run without a GPU."""
 import ctypes as C
@@ -13,7 +14,7 @@ import pytest
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(REPO, "hsi-detectors-cuda_b200", "hsi_b200", "libhsi_b200.so")
 CXXLIB = os.path.join(REPO, "hsi-detectors-cuda_b200", "hsi_b200", "libhsi_cxx.so")
-LIB_OF_HEADER = {"hsi_b200.h": LIB, "hsi_batch.h": CXXLIB}
+LIB_OF_HEADER = {"hsi_b200.h": LIB, "hsi_batch.h": CXXLIB, "hsi_lagged.h": CXXLIB}
 
 
 def declared_symbols(header=None):
