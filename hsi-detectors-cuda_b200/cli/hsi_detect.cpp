@@ -19,6 +19,10 @@
 //                              --threshold is given
 //   --loading=F                diagonal loading of the statistics
 //   --autotune                 time the batch runner's choices on the batch
+//   --lagged                   CEM, RX or ACE with lagged statistics (include/
+//                              hsi_lagged.h): frame k is scored with frame
+//                              k-1's statistics while its own are built on a
+//                              second stream; the RX threshold comes from --pfa
 // Flags are checked before the device is touched, so a usage error exits 2
 // on any machine.  Sources: synthetic, and ENVI replay (--envi, --resident);
 // the HOT snapshot-mosaic directory source is not built and exits 2.
@@ -45,6 +49,7 @@
 #include "hsi/sam_cuda.hpp"
 #include "hsi/spectra_io.hpp"
 #include "hsi_batch.h"
+#include "hsi_lagged.h"
 
 namespace {
 
@@ -85,6 +90,8 @@ Execution
                                 or RX lists), replayed as a CUDA graph
   --repeat=N                    timed replays of the batch                [10]
   --autotune                    time the batch runner's choices first
+  --lagged                      CEM/RX/ACE: score each frame with the previous
+                                frame's statistics, built on a second stream
   --csv=FILE                    write per-frame timings
   --print-detections=N          print the first N detections of the last frame
   --dump-score=FILE             write the last frame's score map as raw float32
@@ -162,7 +169,7 @@ struct Config {
   double loading = 1e-6;
   hsi::PipelineOptions pipeline;
   int frames = 300, warmup = 30, repeat = 10;
-  bool batch = false, autotune = false, quiet = false;
+  bool batch = false, autotune = false, quiet = false, lagged = false;
   std::string csv, dump;
   int print = 0;
 };
@@ -218,6 +225,13 @@ Config configure(const Args& a) {
   c.csv = a.str("csv", a.has("csv") ? "timings.csv" : "");
   c.dump = a.str("dump-score", a.has("dump-score") ? "score.f32" : "");
   c.print = integer(a, "print-detections", 0, 0, 1 << 30);
+  c.lagged = a.has("lagged");
+  if (c.lagged) {
+    if (c.detector == hsi::Detector::Sam) throw UsageError{"--lagged needs --detector=cem, rx or ace"};
+    if (c.batch) throw UsageError{"--lagged and --batch are separate modes"};
+    if (c.detector == hsi::Detector::Rx && c.threshold_given)
+      throw UsageError{"--lagged sets the RX threshold from --pfa; drop --threshold"};
+  }
   if (c.batch) {
     if (c.detector == hsi::Detector::Cem)
       throw UsageError{"--batch lists SAM, ACE and RX detections; run --detector=cem without --batch"};
@@ -426,6 +440,43 @@ int run_stat_stream(const Config& c, hsi::FrameSource* source, const hsi::Spectr
   hsi::DeviceStatistics stats;
   const float* score = c.detector == hsi::Detector::Rx ? d_rx : d_best;
   const std::int32_t* which = c.detector == hsi::Detector::Rx ? nullptr : d_which;
+  // --lagged: the runner holds the maps and lists; frame k scores with frame
+  // k-1's statistics (frame 0 with its own)
+  struct Lagged {
+    hsi_lagged* r = nullptr;
+    ~Lagged() {
+      if (r) hsi_lagged_destroy(r);
+    }
+  } lagged;
+  const int lagged_list = c.detector == hsi::Detector::Cem ? 1 : (c.detector == hsi::Detector::Ace ? 2 : 3);
+  if (c.lagged) {
+    const std::vector<float> flat = library.flatten();
+    hsi_lagged_options o{};
+    o.height = shape.height;
+    o.width = shape.width;
+    o.bands = shape.bands;
+    o.dtype = HSI_F32;
+    o.targets = flat.data();
+    o.num_targets = library.size();
+    o.detectors = c.detector == hsi::Detector::Cem ? HSI_LAGGED_SAM_CEM : HSI_LAGGED_RX_ACE;
+    o.loading = c.loading;
+    o.sam_threshold = 0.10f;
+    o.cem_threshold = static_cast<float>(c.threshold);
+    o.ace_threshold = static_cast<float>(c.threshold);
+    o.rx_false_alarm_rate = c.pfa;
+    o.nms_radius = dp.nms_radius;
+    o.capacity = cap;
+    int st = 0;
+    lagged.r = hsi_lagged_create(&o, &st);
+    if (!lagged.r) {
+      std::fprintf(stderr, "pipeline setup failed: hsi_lagged_create returned %d (%s)\n", st, hsi_status_string(st));
+      return 1;
+    }
+    hsi_lagged_outputs lo{};
+    hsi_lagged_outputs_of(lagged.r, &lo);
+    if (c.detector == hsi::Detector::Rx) dp.threshold = lo.rx_threshold;
+    if (!c.quiet) std::printf("lagged: frame k scored with frame k-1's statistics (frame 0 with its own)\n");
+  }
   Report report;
   std::ofstream csv;
   if (!c.csv.empty()) {
@@ -444,29 +495,49 @@ int run_stat_stream(const Config& c, hsi::FrameSource* source, const hsi::Spectr
     CLI_CUDA(cudaEventRecord(ev[0], s), "event");
     CLI_CUDA(cudaMemcpyAsync(d_cube, h_cube, sizeof(float) * elems, cudaMemcpyHostToDevice, s), "upload");
     CLI_CUDA(cudaEventRecord(ev[1], s), "event");
-    int status = 0;
-    const cudaError_t built = stats.build(d_cube, shape, false, library, c.loading, s, &status);
-    if (built != cudaSuccess) {
-      std::fprintf(stderr, "run failed: statistics of frame %llu: %s (status %d)\n",
-                   static_cast<unsigned long long>(r.meta.index), cudaGetErrorString(built), status);
-      return 1;
+    const hsi::Detection* list = d_out;
+    const unsigned int* list_count = d_count;
+    const float* map = score;
+    if (c.lagged) {
+      CLI_CUDA(cudaEventRecord(ev[2], s), "event");
+      const int st = hsi_lagged_push(lagged.r, d_cube, reinterpret_cast<hsi_stream_t>(s));
+      if (st != HSI_OK) {
+        std::fprintf(stderr, "run failed: lagged frame %llu: %s\n", static_cast<unsigned long long>(r.meta.index),
+                     hsi_status_string(st));
+        return 1;
+      }
+      hsi_lagged_outputs lo{};
+      hsi_lagged_outputs_of(lagged.r, &lo);
+      list = reinterpret_cast<const hsi::Detection*>(lo.detections[lagged_list]);
+      list_count = lo.counts + lagged_list;
+      map = c.detector == hsi::Detector::Rx ? lo.rx : (c.detector == hsi::Detector::Cem ? lo.cem_best : lo.ace_best);
+      CLI_CUDA(cudaEventRecord(ev[3], s), "event");
+      CLI_CUDA(cudaEventRecord(ev[4], s), "event");
+    } else {
+      int status = 0;
+      const cudaError_t built = stats.build(d_cube, shape, false, library, c.loading, s, &status);
+      if (built != cudaSuccess) {
+        std::fprintf(stderr, "run failed: statistics of frame %llu: %s (status %d)\n",
+                     static_cast<unsigned long long>(r.meta.index), cudaGetErrorString(built), status);
+        return 1;
+      }
+      CLI_CUDA(cudaEventRecord(ev[2], s), "event");
+      if (c.detector == hsi::Detector::Cem)
+        CLI_CUDA(hsi::launch_cem(d_cube, shape, false, stats, d_best, d_which, nullptr, P, s), "cem");
+      else
+        CLI_CUDA(hsi::launch_rx_ace(d_cube, shape, false, stats, d_rx, d_best, d_which, nullptr, P, s), "rx/ace");
+      CLI_CUDA(cudaEventRecord(ev[3], s), "event");
+      CLI_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned int), s), "count");
+      CLI_CUDA(hsi::launch_detect(score, which, shape, dp, d_out, d_count, s), "detect");
+      CLI_CUDA(cudaEventRecord(ev[4], s), "event");
     }
-    CLI_CUDA(cudaEventRecord(ev[2], s), "event");
-    if (c.detector == hsi::Detector::Cem)
-      CLI_CUDA(hsi::launch_cem(d_cube, shape, false, stats, d_best, d_which, nullptr, P, s), "cem");
-    else
-      CLI_CUDA(hsi::launch_rx_ace(d_cube, shape, false, stats, d_rx, d_best, d_which, nullptr, P, s), "rx/ace");
-    CLI_CUDA(cudaEventRecord(ev[3], s), "event");
-    CLI_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned int), s), "count");
-    CLI_CUDA(hsi::launch_detect(score, which, shape, dp, d_out, d_count, s), "detect");
-    CLI_CUDA(cudaEventRecord(ev[4], s), "event");
     unsigned int found = 0;
-    CLI_CUDA(cudaMemcpyAsync(&found, d_count, sizeof(found), cudaMemcpyDeviceToHost, s), "download");
+    CLI_CUDA(cudaMemcpyAsync(&found, list_count, sizeof(found), cudaMemcpyDeviceToHost, s), "download");
     CLI_CUDA(cudaStreamSynchronize(s), "download");
     const std::size_t kept = std::min<std::size_t>(found, static_cast<std::size_t>(cap));
     r.detections.resize(kept);
     if (kept)
-      CLI_CUDA(cudaMemcpyAsync(r.detections.data(), d_out, sizeof(hsi::Detection) * kept, cudaMemcpyDeviceToHost, s),
+      CLI_CUDA(cudaMemcpyAsync(r.detections.data(), list, sizeof(hsi::Detection) * kept, cudaMemcpyDeviceToHost, s),
                "download");
     CLI_CUDA(cudaEventRecord(ev[5], s), "event");
     CLI_CUDA(cudaStreamSynchronize(s), "download");
@@ -492,10 +563,12 @@ int run_stat_stream(const Config& c, hsi::FrameSource* source, const hsi::Spectr
     last = std::move(r.detections);
     if (!c.dump.empty() && f == c.warmup + c.frames - 1) {
       last_map.resize(P);
-      CLI_CUDA(cudaMemcpy(last_map.data(), score, sizeof(float) * P, cudaMemcpyDeviceToHost), "score map");
+      CLI_CUDA(cudaMemcpy(last_map.data(), map, sizeof(float) * P, cudaMemcpyDeviceToHost), "score map");
     }
   }
-  report.print(c.detector == hsi::Detector::Cem ? "stats+cem" : "stats+rx/ace", timed_s, shape, false);
+  report.print(c.lagged ? (c.detector == hsi::Detector::Cem ? "lagged cem" : "lagged rx/ace")
+                        : (c.detector == hsi::Detector::Cem ? "stats+cem" : "stats+rx/ace"),
+               timed_s, shape, false);
   if (!c.dump.empty() && !last_map.empty()) dump_map(c.dump, last_map, shape);
   if (c.print > 0) print_detections(last, c.print, unit_of(c.detector));
   return 0;

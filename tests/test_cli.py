@@ -29,7 +29,8 @@ def test_help_lists_the_reference_flags_and_the_added_ones():
     for flag in ["--source=", "--envi=", "--resident=", "--width=", "--height=", "--bands=", "--targets=", "--noise=", "--library=",
                  "--threshold=", "--nms=", "--max-detections=", "--variant=", "--memory=", "--streams=",
                  "--frames=", "--warmup=", "--prefill", "--csv=", "--print-detections=", "--dump-score=",
-                 "--quiet", "--detector=sam|cem|rx|ace", "--batch", "--repeat=", "--pfa=", "--loading="]:
+                 "--quiet", "--detector=sam|cem|rx|ace", "--batch", "--repeat=", "--pfa=", "--loading=",
+                 "--lagged"]:
         assert flag in r.stdout, flag
 
 
@@ -46,6 +47,9 @@ def test_help_lists_the_reference_flags_and_the_added_ones():
     (["--pfa=1.5"], "--pfa must lie in (0, 1)"),
     (["--batch", "--detector=cem"], "--batch lists SAM, ACE and RX detections"),
     (["--batch", "--frames=65"], "--batch takes at most 64 frames"),
+    (["--lagged"], "--lagged needs --detector=cem, rx or ace"),
+    (["--lagged", "--detector=ace", "--batch"], "--lagged and --batch are separate modes"),
+    (["--lagged", "--detector=rx", "--threshold=50"], "--lagged sets the RX threshold from --pfa"),
 ])
 def test_usage_errors_exit_2_before_any_device_call(args, message):
     _build()
@@ -72,6 +76,16 @@ def test_each_detector_runs_end_to_end(detector):
              "--print-detections=2", timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "frames 6 in" in r.stdout and "detections" in r.stdout, r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("detector", ["cem", "rx", "ace"])
+def test_lagged_mode_runs(detector):
+    _build()
+    r = _run("--lagged", f"--detector={detector}", "--width=256", "--height=192", "--bands=64", "--frames=6",
+             "--warmup=2", "--print-detections=2", timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "lagged: frame k scored with frame k-1's statistics" in r.stdout and "frames 6 in" in r.stdout, r.stdout
 
 
 @pytest.mark.gpu
