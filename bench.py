@@ -671,10 +671,94 @@ def same_shape_scorer(hsi, torch, device, passes=5, iterations=50, warm_s=0.5):
             "results": out}
 
 
+def lagged_record(hsi, torch, device, frames=16, warm=3):
+    """The SAM+CEM video step of the headline workload in the lagged-statistics
+    mode (include/hsi_lagged.h): each 1024x1024x113 frame is scored with the
+    previous frame's statistics while its own are built on a second stream,
+    against the same frames each scored with its own statistics, one frame at
+    a time on one stream.  Per-frame time in steady state, and the latency of
+    a frame (its work on the scoring stream: statistics first, or not)."""
+    import ctypes as C
+    L = hsi.lib()
+    sc = hsi.scene(B, n_targets=TARGETS, target_frac=0.002, library_seed=0x5EED1000)
+    targets_np = hsi.scene_targets(sc)
+    cubes = []
+    for f in range(frames):
+        s_ = hsi.scene(B, n_targets=TARGETS, target_frac=0.002, library_seed=0x5EED1000, frame_seed=0x5EED1000 + f)
+        cubes.append(hsi.generate(s_, H, W, truth=False, device=device)[0])
+    stream = torch.cuda.current_stream(device)
+    run = hsi.Lagged(H, W, B, targets_np, detectors=hsi.LAGGED_SAM_CEM, loading=LOADING, sam_threshold=THRESHOLD,
+                     cem_threshold=CEM_THRESHOLD, nms_radius=NMS_RADIUS, capacity=CAPACITY)
+
+    def timed(push):
+        for f in range(warm):
+            push(cubes[f])
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(frames)]
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for f in range(frames):
+            ev[f][0].record(stream)
+            push(cubes[f])
+            ev[f][1].record(stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / frames
+        lat = float(np.median([x.elapsed_time(y) for x, y in ev]))
+        return ms, lat
+
+    lag_ms, lag_lat = timed(lambda c: run.push(c, stream))
+    # the same frames, each on its own statistics, one frame at a time
+    P = H * W
+    tg = torch.from_numpy(targets_np).to(device)
+    nr = torch.from_numpy(hsi.target_norms(targets_np)).to(device)
+    moments = torch.zeros(B + B * B + 1, dtype=torch.float64, device=device)
+    cem_w = torch.zeros((TARGETS, B), device=device)
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    sws_b = L.hsi_stats_workspace_bytes(H, W, B)
+    sws = torch.empty(sws_b, dtype=torch.uint8, device=device)
+    smaps = torch.empty((TARGETS, P), device=device)
+    cmaps = torch.empty((TARGETS, P), device=device)
+    best = [torch.empty(P, device=device) for _ in range(2)]
+    bt = [torch.empty(P, dtype=torch.int32, device=device) for _ in range(2)]
+    dets = torch.empty((2, CAPACITY, 4), dtype=torch.int32, device=device)
+    counts = torch.zeros(2, dtype=torch.int32, device=device)
+    jobs = [hsi.detect_job(best[0], bt[0], H, W, THRESHOLD, NMS_RADIUS, hsi.LOWER_IS_BETTER, CAPACITY, dets[0],
+                           counts[0:1]),
+            hsi.detect_job(best[1], bt[1], H, W, CEM_THRESHOLD, NMS_RADIUS, hsi.HIGHER_IS_BETTER, CAPACITY, dets[1],
+                           counts[1:2])]
+    dws = torch.empty(hsi.detect_batch_workspace_bytes(jobs), dtype=torch.uint8, device=device)
+    s = C.c_void_p(stream.cuda_stream)
+    vp = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+
+    def own(cube):
+        stride = cube.shape[-1]
+        hsi.check(L.hsi_scene_moments(vp(cube), H, W, B, 0, stride, vp(moments), None, vp(sws), sws_b, s), "moments")
+        hsi.check(L.hsi_build_statistics(1, B, TARGETS, LOADING, vp(moments), vp(tg), 0, None, None, vp(cem_w),
+                                         vp(status), None, 0, s), "statistics")
+        hsi.score_frames([hsi.make_frame(cube, H, W, B, 0, sam_targets=tg, sam_norms=nr, cem_weights=cem_w,
+                                         sam_maps=smaps, sam_best=best[0], sam_best_target=bt[0], cem_maps=cmaps,
+                                         cem_best=best[1], cem_best_target=bt[1], map_stride=P)], stream=stream)
+        counts.zero_()
+        hsi.detect_batch(jobs, dws, stream=stream)
+
+    own_ms, own_lat = timed(own)
+    run.close()
+    del cubes, sws, smaps, cmaps, best, bt, dets, dws
+    torch.cuda.empty_cache()
+    return {"what": f"{frames} frames of {H}x{W}x{B} f32, {TARGETS} targets, SAM+CEM maps and both lists, pushed "
+                    "one at a time (median latency = the frame's work on the scoring stream)",
+            "lagged": {"ms_per_frame": round(lag_ms, 3), "mpix_s": round(P / (lag_ms / 1e3) / 1e6, 1),
+                       "latency_ms": round(lag_lat, 3)},
+            "own_statistics": {"ms_per_frame": round(own_ms, 3), "mpix_s": round(P / (own_ms / 1e3) / 1e6, 1),
+                               "latency_ms": round(own_lat, 3)}}
+
+
 def extra_records(args, device, line):
     """The default run's other records, each measured after the headline
-    (single GPU only): the RX+ACE precision workload, the learned screen, and
-    the SAM scorer at the shapes of the reference's GPU comparator."""
+    (single GPU only): the RX+ACE precision workload, the learned screen, the
+    SAM scorer at the shapes of the reference's GPU comparator, and the
+    SAM+CEM video in the lagged-statistics mode."""
     import torch
     import hsi_b200 as hsi
     sub = argparse.Namespace(**vars(args))
@@ -691,6 +775,10 @@ def extra_records(args, device, line):
         line["same_shape_scorer"] = same_shape_scorer(hsi, torch, device)
     except Exception as e:
         line["same_shape_scorer"] = {"error": f"{type(e).__name__}: {e}"}
+    try:
+        line["lagged_statistics"] = lagged_record(hsi, torch, device)
+    except Exception as e:
+        line["lagged_statistics"] = {"error": f"{type(e).__name__}: {e}"}
 
 
 # DRAM bytes (read + write) per frame of the scoring kernel, from the ncu
