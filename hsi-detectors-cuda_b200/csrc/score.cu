@@ -20,8 +20,8 @@
 // reduction src/detectors_cpu.cpp:158-187.
 #include <cuda_fp16.h>
 
-#include <mutex>
 
+#include "launch_state.h"
 #include "tc.cuh"
 
 namespace hsi_b200 {
@@ -1158,16 +1158,7 @@ __global__ void __launch_bounds__(kHThreads, 1) score_h_kernel(const __grid_cons
 // Host side
 // ---------------------------------------------------------------------------
 
-int sm_count() {
-  // read once per process (a local static's initialisation is thread-safe)
-  static const int n = [] {
-    int dev = 0, v = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
-    return v > 0 ? v : 148;
-  }();
-  return n;
-}
+int sm_count() { return device_sm_count(); }
 
 constexpr int kSupported[] = {0, 1, 4, 8, 16};
 
@@ -1183,26 +1174,13 @@ int launch_instance(const ScoreParams& p, int max_bands, int ctas_per_sm, cudaSt
   const SmemLayout L = smem_layout<T>(kGroups, max_bands, score_slots<KS, KC>(), score_stages<T, KS, KC>());
   const int threads = kGroups * kGroupThreads + 32;
   auto kernel = score_kernel<T, KS, KC>;
-  // The attribute and the residency follow the band count of the call; the
-  // lock keeps the pair consistent when host threads launch concurrently.
-  static std::mutex mu;
-  static int configured_bytes = -1;
-  static int configured_per_sm = 0;
-  int per_sm = 0;
-  {
-    const std::lock_guard<std::mutex> lock(mu);
-    if (configured_bytes != static_cast<int>(L.total)) {
-      cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast<int>(L.total));
-      if (e != cudaSuccess) return static_cast<int>(e);
-      int v = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, threads, L.total);
-      if (e != cudaSuccess) return static_cast<int>(e);
-      configured_per_sm = v < 1 ? 1 : v;
-      configured_bytes = static_cast<int>(L.total);
-    }
-    per_sm = configured_per_sm;
-  }
+  // The layout follows the band count of the call.  The device's limit for
+  // this kernel only ever rises, so a concurrent call with fewer bands cannot
+  // lower it below this launch's layout; residency is per layout and device.
+  const cudaError_t e = raise_smem_limit(kernel, static_cast<int>(L.total));
+  if (e != cudaSuccess) return static_cast<int>(e);
+  const int resident = device_residency(kernel, threads, L.total);
+  const int per_sm = resident < 1 ? 1 : resident;
   // ctas_per_sm: 0 = as many as fit; otherwise that many (capped at what fits)
   const int per = ctas_per_sm > 0 && ctas_per_sm < per_sm ? ctas_per_sm : per_sm;
   const int grid = sm_count() * per;
@@ -1276,10 +1254,8 @@ int launch_h(const HParams& p, cudaStream_t stream) {
   constexpr int N2 = 2 * ((KS + KC + 15) / 16 * 16);
   auto kernel = score_h_kernel<KS, KC>;
   const HSmem L = h_smem(p.bp, N2);
-  // set once per process, at the largest layout (a local static's
-  // initialisation is thread-safe)
-  static const cudaError_t configured = cudaFuncSetAttribute(
-      kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(h_smem(kHMaxBands, N2).total));
+  // the largest layout, set once per device
+  const cudaError_t configured = raise_smem_limit(kernel, static_cast<int>(h_smem(kHMaxBands, N2).total));
   if (configured != cudaSuccess) return static_cast<int>(configured);
   kernel<<<sm_count(), kHThreads, L.total, stream>>>(p);
   return static_cast<int>(cudaGetLastError());
@@ -1312,7 +1288,7 @@ bool tensor_core_frame(const hsi_frame& f) {
 // (128-byte swizzle, boxes of 64 pixels x all bands) per cube, one launch per
 // pass.
 int score_h_group(const hsi_frame* const* frames, int n, int* status, cudaStream_t s) {
-  static HParams p;  // 16 KB: kept off the stack; the launch copies it
+  static thread_local HParams p;  // 16 KB: kept off the stack, one per host thread; the launch copies it
   p = HParams{};
   p.num_frames = n;
   p.status = status;
@@ -1343,7 +1319,7 @@ int score_h_group(const hsi_frame* const* frames, int n, int* status, cudaStream
 
 // FP32-FMA scorer over up to 64 validated frames of one element type.
 int score_fma_group(const hsi_frame* const* frames, int n, int* status, cudaStream_t s) {
-  static ScoreParams p;  // 8 KB: kept off the stack; the launch copies it
+  static thread_local ScoreParams p;  // 8 KB: kept off the stack, one per host thread; the launch copies it
   p = ScoreParams{};
   p.table = nullptr;
   p.num_frames = n;
@@ -1358,8 +1334,6 @@ int score_fma_group(const hsi_frame* const* frames, int n, int* status, cudaStre
   return run_passes(p, frames[0]->dtype, max_bands, max_sam, max_cem, 0, s);
 }
 
-std::mutex g_host_frames_mutex;  // the group launchers keep their parameter blocks in statics
-
 // Frames whose descriptors are on the host: FP16 cubes of at most 128 bands
 // go to the tensor-core scorer, the rest to the FP32-FMA scorer, 64 frames
 // per launch.
@@ -1369,7 +1343,6 @@ int score_host_frames(const hsi_frame* frames, int n, int* status, cudaStream_t 
     const int rc = validate_frame(frames[i]);
     if (rc != HSI_OK) return rc;
   }
-  std::lock_guard<std::mutex> lock(g_host_frames_mutex);
   const hsi_frame* group[3][kMaxInline];  // tensor-core fp16, FMA fp32, FMA fp16
   int count[3] = {0, 0, 0};
   auto flush = [&](int g) -> int {
