@@ -11,12 +11,16 @@
 //   R = M2/N + loading I = C C^T,  x_t = R^-1 d_t,  w_t = x_t / (d_t . x_t)
 //                                              (CEM; 0 if d_t . x_t <= 0)
 // All arithmetic is FP64, because the factorisation of a nearly rank-6
-// covariance needs it.  One CTA per frame; frames of a batch factor in
+// covariance needs it.  One cluster of two CTAs per frame: the covariance and
+// the correlation chains run at once on two SMs; frames of a batch factor in
 // parallel.  Matrices live in shared memory as packed lower triangles when
-// they fit (B <= 128) and in the caller's workspace otherwise.  The solves use
-// the explicit triangular inverses (blocked, parallel) rather than sequential
-// substitution, so a single frame factors in ~0.1 ms instead of being bound by
-// ~10^4 dependent FP64 steps.
+// they fit (B <= 128) and in the caller's workspace otherwise.  The
+// factorisation and the triangular inverse are blocked (16-column panels, the
+// diagonal blocks factored and inverted by one warp in registers), and the
+// solves use the explicit inverses, so no chain of ~B dependent steps with a
+// block barrier each remains.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace hsi_b200 {
@@ -26,10 +30,17 @@ constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSmemMaxBands = 128;
 constexpr int kChunk = 16;  // targets per pass through the per-target buffers
-constexpr int kBlk = 16;    // row block of the triangular inverse
+constexpr int kNb = 16;     // panel width of the blocked factorisation
+constexpr int kLpStride = kNb + 1;  // doubles per panel row in shared memory (spreads the banks)
 
 __host__ __device__ inline size_t tri(int n) { return static_cast<size_t>(n) * (n + 1) / 2; }
 __device__ __forceinline__ size_t row_off(int i) { return static_cast<size_t>(i) * (i + 1) / 2; }
+// doubles of the panel buffer (n rows of kLpStride), which the inverse reuses
+// as its block-row buffer (kNb rows of up to n columns)
+__host__ __device__ inline size_t lp_elems(int n) {
+  const size_t a = static_cast<size_t>(n) * (kNb + 1), b = static_cast<size_t>(kNb) * n;
+  return a > b ? a : b;
+}
 
 struct FactorArgs {
   int bands, targets;
@@ -67,63 +78,155 @@ __device__ void fill_matrix(double* A, const double* outer, const double* mean, 
   __syncthreads();
 }
 
-// In-place right-looking Cholesky of a packed lower triangle, one barrier per
-// elimination step: step k subtracts a_ik a_jk / a_kk from the trailing
-// triangle with the column left unscaled, and all columns are scaled by
-// 1/sqrt(pivot) at the end.  Returns false -- the same on every thread, which
-// all read the same pivot -- if a pivot is not positive or is NaN
-// (src/linalg.cpp:105-122).  `dv`: n doubles of scratch.
-__device__ bool cholesky_packed(double* a, int n, double* dv) {
+// ---- blocked Cholesky and triangular inverse (panels of kNb columns) --------
+//
+// The unblocked factorisation is a chain of n dependent steps, each paying a
+// block barrier, a pivot read and an FP64 division.  Blocked, the chain is
+// n / kNb panels.  Per panel:
+//   1. one warp factors the kNb x kNb diagonal block in registers (shuffles,
+//      no barriers) and inverts its factor, V = L_kk^-1, the same way;
+//   2. all threads form the panel below it, L_21 = A_21 V^T (independent
+//      16-term dot products: the triangular solve becomes a product);
+//   3. all threads update the trailing triangle, A_22 -= L_21 L_21^T.
+// The inverse W = L^-1 then goes by block rows: W_II = V_II (kept from step
+// 1), and W_IJ = -V_II sum_{K=J}^{I-1} L_IK W_KJ for all J < I at once.
+
+// Step 1 (one warp): factor the diagonal block at k0 (kb <= kNb rows) in
+// registers, lane l holding row l.  Writes L_kk into A, V = L_kk^-1 into W's
+// diagonal block and densely into vs[row * kNb + col].  Sets *bad if a pivot
+// is not positive (or NaN).
+__device__ void diag_block(double* A, double* W, double* vs, int k0, int kb, int* bad) {
+  const int l = threadIdx.x & 31;
+  constexpr unsigned kAll = 0xffffffffu;
+  double a[kNb];
+#pragma unroll
+  for (int m = 0; m < kNb; ++m) a[m] = (l < kb && m <= l) ? A[row_off(k0 + l) + k0 + m] : 0.0;
+  double rd[kNb];
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < kNb; ++k) {
+    rd[k] = 0.0;
+    if (k < kb) {
+      const double akk = __shfl_sync(kAll, a[k], k);
+      ok = ok && akk > 0.0;
+      const double sq = sqrt(akk);
+      const double inv = 1.0 / sq;
+      rd[k] = inv;
+      if (l == k) a[k] = sq;
+      else if (l > k) a[k] *= inv;
+#pragma unroll
+      for (int j = k + 1; j < kNb; ++j) {
+        const double ljk = __shfl_sync(kAll, a[k], j);
+        if (l >= j) a[j] -= a[k] * ljk;
+      }
+    }
+  }
+  // V = L^-1, lane l computing column l by forward substitution
+  double v[kNb];
+#pragma unroll
+  for (int i = 0; i < kNb; ++i) {
+    double t = i == l ? 1.0 : 0.0;
+#pragma unroll
+    for (int m = 0; m < i; ++m) t -= __shfl_sync(kAll, a[m], i) * v[m];
+    v[i] = (i >= l && i < kb) ? t * rd[i] : 0.0;
+  }
+  if (l < kb) {
+    double* ar = A + row_off(k0 + l) + k0;
+#pragma unroll
+    for (int m = 0; m < kNb; ++m)
+      if (m <= l) ar[m] = a[m];
+  }
+  if (l < kNb) {
+#pragma unroll
+    for (int i = 0; i < kNb; ++i) {
+      vs[i * kNb + l] = v[i];
+      if (i >= l && i < kb && l < kb) W[row_off(k0 + i) + k0 + l] = v[i];
+    }
+  }
+  if (!ok && l == 0) *bad = 1;
+}
+
+// In-place blocked Cholesky of a packed lower triangle (src/linalg.cpp:105-122):
+// A holds L on return, and W's diagonal blocks hold their inverses.  Returns
+// false -- on every thread -- if a pivot is not positive or is NaN.
+// lp: n * kLpStride doubles; vs: kNb * kNb; bad: a shared int.
+__device__ bool cholesky_blocked(double* A, double* W, int n, double* lp, double* vs, int* bad) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int k = 0; k < n; ++k) {
-    const double d = a[row_off(k) + k];
-    if (!(d > 0.0)) return false;
-    const double inv = 1.0 / d;
-    for (int i = k + 1 + warp; i < n; i += kWarps) {
-      double* ri = a + row_off(i);
-      const double f = ri[k] * inv;
-      for (int j = k + 1 + lane; j <= i; j += 32) ri[j] -= f * a[row_off(j) + k];
+  if (threadIdx.x == 0) *bad = 0;
+  __syncthreads();
+  for (int k0 = 0; k0 < n; k0 += kNb) {
+    const int kb = min(kNb, n - k0);
+    if (warp == 0) diag_block(A, W, vs, k0, kb, bad);
+    __syncthreads();
+    if (*bad) return false;
+    const int r0 = k0 + kb;
+    const int rows = n - r0;
+    if (rows == 0) break;
+    // panel: lp[i][j] = sum_{m <= j} A[r0 + i][k0 + m] V[j][m]  (kb == kNb here)
+    for (int e = threadIdx.x; e < rows * kNb; e += blockDim.x) {
+      const int i = e / kNb, j = e % kNb;
+      const double* ai = A + row_off(r0 + i) + k0;
+      const double* vj = vs + j * kNb;
+      double t = 0.0;
+      for (int m = 0; m <= j; ++m) t += ai[m] * vj[m];
+      lp[i * kLpStride + j] = t;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < rows * kNb; e += blockDim.x) {
+      const int i = e / kNb, j = e % kNb;
+      A[row_off(r0 + i) + k0 + j] = lp[i * kLpStride + j];
+    }
+    // trailing triangle: A[r0 + i][r0 + j] -= lp[i] . lp[j], j <= i
+    for (int i = warp; i < rows; i += kWarps) {
+      const double* li = lp + i * kLpStride;
+      double* ai = A + row_off(r0 + i) + r0;
+      for (int j = lane; j <= i; j += 32) {
+        const double* lj = lp + j * kLpStride;
+        double t = 0.0;
+#pragma unroll
+        for (int m = 0; m < kNb; ++m) t += li[m] * lj[m];
+        ai[j] -= t;
+      }
     }
     __syncthreads();
   }
-  for (int k = threadIdx.x; k < n; k += blockDim.x) dv[k] = sqrt(a[row_off(k) + k]);
-  __syncthreads();
-  for (int i = warp; i < n; i += kWarps) {
-    double* ri = a + row_off(i);
-    for (int j = lane; j <= i; j += 32) ri[j] = j == i ? dv[i] : ri[j] / dv[j];
-  }
-  __syncthreads();
   return true;
 }
 
-// Winv = L^-1 (both packed lower) by blocked forward substitution on L X = I
-// (src/linalg.cpp:150-162 solves the same system column by column).  Per row
-// block [r0, r1): first every (row, column) takes the part of its sum over the
-// finished rows j < r0 in parallel, then each thread finishes one column down
-// the block's rows.
-__device__ void triangular_inverse(const double* L, double* Winv, int n) {
-  for (int r0 = 0; r0 < n; r0 += kBlk) {
-    const int r1 = min(r0 + kBlk, n);
-    const int work = (r1 - r0) * r1;
-    for (int e = threadIdx.x; e < work; e += blockDim.x) {
-      const int i = r0 + e / r1, c = e % r1;
-      if (c > i) continue;
-      double s = c == i ? 1.0 : 0.0;
-      if (c < r0) {
-        const double* li = L + row_off(i);
-        for (int j = c; j < r0; ++j) s -= li[j] * Winv[row_off(j) + c];
+// W = L^-1 (both packed lower) by block rows, given L and the inverses of its
+// diagonal blocks already in W (src/linalg.cpp:150-162 solves the same system
+// column by column).  tb: kNb * n doubles.  Each thread of phase 1 takes one
+// column and four rows of the block row, so a W element read from shared
+// memory serves four products.
+__device__ void inverse_blocked(const double* L, double* W, int n, double* tb) {
+  constexpr int kRows = 4;
+  for (int i0 = kNb; i0 < n; i0 += kNb) {
+    const int ib = min(kNb, n - i0);
+    const int groups = (ib + kRows - 1) / kRows;
+    // phase 1: tb[r][c] = sum_{m=c}^{i0-1} L[i0 + r][m] W[m][c],  r < ib, c < i0
+    for (int e = threadIdx.x; e < groups * i0; e += blockDim.x) {
+      const int g = e / i0, c = e % i0;
+      double t[kRows] = {0.0, 0.0, 0.0, 0.0};
+      const double* lr[kRows];
+#pragma unroll
+      for (int q = 0; q < kRows; ++q) lr[q] = L + row_off(i0 + min(g * kRows + q, ib - 1));
+      for (int m = c; m < i0; ++m) {
+        const double w = W[row_off(m) + c];
+#pragma unroll
+        for (int q = 0; q < kRows; ++q) t[q] += lr[q][m] * w;
       }
-      Winv[row_off(i) + c] = s;
+#pragma unroll
+      for (int q = 0; q < kRows; ++q)
+        if (g * kRows + q < ib) tb[(g * kRows + q) * i0 + c] = t[q];
     }
     __syncthreads();
-    for (int c = threadIdx.x; c < r1; c += blockDim.x) {
-      const int j0 = max(r0, c);
-      for (int i = j0; i < r1; ++i) {
-        const double* li = L + row_off(i);
-        double s = Winv[row_off(i) + c];
-        for (int j = j0; j < i; ++j) s -= li[j] * Winv[row_off(j) + c];
-        Winv[row_off(i) + c] = s / li[i];
-      }
+    // phase 2: W[i0 + r][c] = -sum_{m <= r} V[r][m] tb[m][c]
+    for (int e = threadIdx.x; e < ib * i0; e += blockDim.x) {
+      const int r = e / i0, c = e % i0;
+      const double* vr = W + row_off(i0 + r) + i0;
+      double t = 0.0;
+      for (int m = 0; m <= r; ++m) t += vr[m] * tb[m * i0 + c];
+      W[row_off(i0 + r) + c] = -t;
     }
     __syncthreads();
   }
@@ -154,9 +257,20 @@ __device__ void upper_matvec(const double* M, const double* v, double* out, int 
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kThreads) factor_kernel(const FactorArgs args) {
+// One cluster of two CTAs per frame, on two SMs at once:
+//   rank 0: covariance S = L L^T -> mean, whitener W = L^-1, ACE vectors;
+//   rank 1: correlation R = C C^T -> CEM weights (only when there are targets).
+// The chains share nothing but the mean, which each computes.  At the end
+// rank 1 writes its result code into rank 0's shared memory and rank 0 writes
+// the frame's status: an empty frame or a covariance that is not positive
+// definite first (the reference stops there), else the correlation's code.
+__global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(kThreads) factor_kernel(const FactorArgs args) {
+  namespace cg = cooperative_groups;
   extern __shared__ double smem[];
+  __shared__ int s_partner_code;
+  __shared__ int s_bad;
   const int f = blockIdx.x;
+  const int chain = blockIdx.y;  // 0: covariance, 1: correlation
   const int B = args.bands, T = args.targets;
   const double* mom = args.moments + f * args.moments_stride;
   const float* lib = args.library ? args.library + f * args.library_stride : nullptr;
@@ -165,107 +279,106 @@ __global__ void __launch_bounds__(kThreads) factor_kernel(const FactorArgs args)
   float* out32 = args.stats32 ? args.stats32 + f * per : nullptr;
   float* cem32 = args.cem32 ? args.cem32 + static_cast<size_t>(f) * T * B : nullptr;
   const bool in_smem = B <= kSmemMaxBands;
-  // smem: mean[B], pivots[B], two chunk buffers of kChunk x B, then the
-  // packed matrices (in the workspace when B is large)
+  // smem: mean[B], two chunk buffers of kChunk x B, the panel / block-row
+  // buffer, the diagonal block's inverse, then the packed matrices (in the
+  // workspace when B is large)
   double* mean = smem;
-  double* dv = mean + B;
-  double* vec = dv + B;
+  double* vec = mean + B;
   double* buf = vec + static_cast<size_t>(kChunk) * B;
-  double* A = in_smem ? buf + static_cast<size_t>(kChunk) * B : args.scratch + static_cast<size_t>(f) * 2 * tri(B);
+  double* lp = buf + static_cast<size_t>(kChunk) * B;
+  double* vs = lp + lp_elems(B);
+  double* A = in_smem ? vs + kNb * kNb : args.scratch + (static_cast<size_t>(f) * 2 + chain) * 2 * tri(B);
   double* W = A + tri(B);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-  const double N = mom[B + B * B];
-  if (!(N > 0.0)) {
-    if (threadIdx.x == 0 && args.status) args.status[f] = HSI_E_EMPTY;
-    return;
-  }
-  const double* sum = mom;
-  const double* outer = mom + B;
-  for (int i = threadIdx.x; i < B; i += blockDim.x) mean[i] = sum[i] / N;
-  __syncthreads();
-  // covariance, loaded (src/linalg.cpp:56-79), its Cholesky factor and inverse
-  fill_matrix(A, outer, mean, N, args.loading, B, true);
-  if (!cholesky_packed(A, B, dv)) {
-    if (threadIdx.x == 0 && args.status) args.status[f] = HSI_E_NOT_POSITIVE_DEFINITE;
-    return;
-  }
-  triangular_inverse(A, W, B);
-  // outputs: mean, whitener (row-major, upper zero)
-  for (int i = threadIdx.x; i < B; i += blockDim.x) {
-    if (out64) out64[i] = mean[i];
-    if (out32) out32[i] = static_cast<float>(mean[i]);
-  }
-  for (size_t e = threadIdx.x; e < static_cast<size_t>(B) * B; e += blockDim.x) {
-    const int i = static_cast<int>(e / B), j = static_cast<int>(e % B);
-    const double v = j <= i ? W[row_off(i) + j] : 0.0;
-    if (out64) out64[B + e] = v;
-    if (out32) out32[B + e] = static_cast<float>(v);
-  }
-  if (T == 0) {
-    if (threadIdx.x == 0 && args.status) args.status[f] = HSI_OK;
-    return;
-  }
   const size_t off_tw = static_cast<size_t>(B) + static_cast<size_t>(B) * B;
   const size_t off_tn = off_tw + static_cast<size_t>(T) * B;
   const size_t off_cw = off_tn + T;
-  // ACE: u_t = W (d_t - mu) and |u_t|^2, kChunk targets at a time
-  for (int t0 = 0; t0 < T; t0 += kChunk) {
-    const int nt = min(kChunk, T - t0);
-    for (int e = threadIdx.x; e < nt * B; e += blockDim.x)
-      vec[e] = static_cast<double>(lib[static_cast<size_t>(t0) * B + e]) - mean[e % B];
+
+  int code = HSI_OK;
+  const double N = mom[B + B * B];
+  const double* sum = mom;
+  const double* outer = mom + B;
+  if (!(N > 0.0)) code = HSI_E_EMPTY;
+  if (code == HSI_OK && (chain == 0 || T > 0)) {
+    for (int i = threadIdx.x; i < B; i += blockDim.x) mean[i] = sum[i] / N;
     __syncthreads();
-    lower_matvec(W, vec, buf, B, nt);
-    for (int e = threadIdx.x; e < nt * B; e += blockDim.x) {
-      if (out64) out64[off_tw + static_cast<size_t>(t0) * B + e] = buf[e];
-      if (out32) out32[off_tw + static_cast<size_t>(t0) * B + e] = static_cast<float>(buf[e]);
-    }
-    for (int t = warp; t < nt; t += kWarps) {
-      double s = 0.0;
-      for (int i = lane; i < B; i += 32) s += buf[t * B + i] * buf[t * B + i];
-      s = warp_sum(s);
-      if (lane == 0) {
-        if (out64) out64[off_tn + t0 + t] = s;
-        if (out32) out32[off_tn + t0 + t] = static_cast<float>(s);
+    // covariance (chain 0) or correlation (chain 1), loaded (src/linalg.cpp:56-79)
+    fill_matrix(A, outer, mean, N, args.loading, B, chain == 0);
+    if (!cholesky_blocked(A, W, B, lp, vs, &s_bad)) {
+      code = chain == 0 ? HSI_E_NOT_POSITIVE_DEFINITE : HSI_E_CORRELATION_NOT_PD;
+    } else {
+      inverse_blocked(A, W, B, lp);
+      if (chain == 0) {
+        // outputs: mean, whitener (row-major, upper zero)
+        for (int i = threadIdx.x; i < B; i += blockDim.x) {
+          if (out64) out64[i] = mean[i];
+          if (out32) out32[i] = static_cast<float>(mean[i]);
+        }
+        for (size_t e = threadIdx.x; e < static_cast<size_t>(B) * B; e += blockDim.x) {
+          const int i = static_cast<int>(e / B), j = static_cast<int>(e % B);
+          const double v = j <= i ? W[row_off(i) + j] : 0.0;
+          if (out64) out64[B + e] = v;
+          if (out32) out32[B + e] = static_cast<float>(v);
+        }
+        // ACE: u_t = W (d_t - mu) and |u_t|^2, kChunk targets at a time
+        for (int t0 = 0; t0 < T; t0 += kChunk) {
+          const int nt = min(kChunk, T - t0);
+          for (int e = threadIdx.x; e < nt * B; e += blockDim.x)
+            vec[e] = static_cast<double>(lib[static_cast<size_t>(t0) * B + e]) - mean[e % B];
+          __syncthreads();
+          lower_matvec(W, vec, buf, B, nt);
+          for (int e = threadIdx.x; e < nt * B; e += blockDim.x) {
+            if (out64) out64[off_tw + static_cast<size_t>(t0) * B + e] = buf[e];
+            if (out32) out32[off_tw + static_cast<size_t>(t0) * B + e] = static_cast<float>(buf[e]);
+          }
+          for (int t = warp; t < nt; t += kWarps) {
+            double q = 0.0;
+            for (int i = lane; i < B; i += 32) q += buf[t * B + i] * buf[t * B + i];
+            q = warp_sum(q);
+            if (lane == 0) {
+              if (out64) out64[off_tn + t0 + t] = q;
+              if (out32) out32[off_tn + t0 + t] = static_cast<float>(q);
+            }
+          }
+          __syncthreads();
+        }
+      } else {
+        // CEM: y_t = C^-1 d_t, x_t = C^-T y_t = R^-1 d_t, d_t . x_t = |y_t|^2;
+        // w_t = x_t / |y_t|^2, 0 if that gain is not positive (src/detector.cpp:128-148)
+        for (int t0 = 0; t0 < T; t0 += kChunk) {
+          const int nt = min(kChunk, T - t0);
+          for (int e = threadIdx.x; e < nt * B; e += blockDim.x)
+            vec[e] = static_cast<double>(lib[static_cast<size_t>(t0) * B + e]);
+          __syncthreads();
+          lower_matvec(W, vec, buf, B, nt);   // y
+          upper_matvec(W, buf, vec, B, nt);   // x (d is no longer needed)
+          for (int t = warp; t < nt; t += kWarps) {
+            double g = 0.0;
+            for (int i = lane; i < B; i += 32) g += buf[t * B + i] * buf[t * B + i];
+            g = warp_sum(g);
+            for (int i = lane; i < B; i += 32) {
+              const double w = g > 0.0 ? vec[t * B + i] / g : 0.0;
+              const size_t o = static_cast<size_t>(t0 + t) * B + i;
+              if (out64) out64[off_cw + o] = w;
+              if (out32) out32[off_cw + o] = static_cast<float>(w);
+              if (cem32) cem32[o] = static_cast<float>(w);
+            }
+          }
+          __syncthreads();
+        }
       }
     }
-    __syncthreads();
   }
-  // CEM: R = M2/N + loading I = C C^T; y_t = C^-1 d_t, x_t = C^-T y_t = R^-1 d_t,
-  // d_t . x_t = |y_t|^2; w_t = x_t / |y_t|^2, 0 if that gain is not positive
-  // (src/detector.cpp:128-148)
-  fill_matrix(A, outer, mean, N, args.loading, B, false);
-  if (!cholesky_packed(A, B, dv)) {
-    if (threadIdx.x == 0 && args.status) args.status[f] = HSI_E_CORRELATION_NOT_PD;
-    return;
-  }
-  triangular_inverse(A, W, B);
-  for (int t0 = 0; t0 < T; t0 += kChunk) {
-    const int nt = min(kChunk, T - t0);
-    for (int e = threadIdx.x; e < nt * B; e += blockDim.x)
-      vec[e] = static_cast<double>(lib[static_cast<size_t>(t0) * B + e]);
-    __syncthreads();
-    lower_matvec(W, vec, buf, B, nt);   // y
-    upper_matvec(W, buf, vec, B, nt);   // x (d is no longer needed)
-    for (int t = warp; t < nt; t += kWarps) {
-      double g = 0.0;
-      for (int i = lane; i < B; i += 32) g += buf[t * B + i] * buf[t * B + i];
-      g = warp_sum(g);
-      for (int i = lane; i < B; i += 32) {
-        const double w = g > 0.0 ? vec[t * B + i] / g : 0.0;
-        const size_t o = static_cast<size_t>(t0 + t) * B + i;
-        if (out64) out64[off_cw + o] = w;
-        if (out32) out32[off_cw + o] = static_cast<float>(w);
-        if (cem32) cem32[o] = static_cast<float>(w);
-      }
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0 && args.status) args.status[f] = HSI_OK;
+  // combine the two chains' codes in rank 0 (every thread of both CTAs
+  // reaches the cluster barrier: no early returns above)
+  cg::cluster_group cluster = cg::this_cluster();
+  if (chain == 1 && threadIdx.x == 0) *cluster.map_shared_rank(&s_partner_code, 0) = code;
+  cluster.sync();
+  if (chain == 0 && threadIdx.x == 0 && args.status) args.status[f] = code != HSI_OK ? code : s_partner_code;
 }
 
 size_t smem_bytes(int B, int /*T*/) {
-  const size_t vectors = 2 * static_cast<size_t>(B) + 2 * static_cast<size_t>(kChunk) * B;
+  const size_t vectors = static_cast<size_t>(B) + 2 * static_cast<size_t>(kChunk) * B + lp_elems(B) + kNb * kNb;
   if (B <= kSmemMaxBands) return sizeof(double) * (vectors + 2 * tri(B));
   return sizeof(double) * vectors;
 }
@@ -284,7 +397,8 @@ extern "C" HSI_API size_t hsi_statistics_elements(int bands, int num_targets) {
 extern "C" HSI_API size_t hsi_factor_workspace_bytes(int num_frames, int bands) {
   if (num_frames <= 0 || bands <= 0) return 0;
   if (bands <= kSmemMaxBands) return 0;
-  return sizeof(double) * 2 * tri(bands) * static_cast<size_t>(num_frames);
+  // both chains' matrices (A and W) per frame
+  return sizeof(double) * 4 * tri(bands) * static_cast<size_t>(num_frames);
 }
 
 extern "C" HSI_API int hsi_build_statistics(int num_frames, int bands, int num_targets, double loading,
@@ -316,6 +430,6 @@ extern "C" HSI_API int hsi_build_statistics(int num_frames, int bands, int num_t
   cudaError_t e = cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return static_cast<int>(e);
-  factor_kernel<<<num_frames, kThreads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(a);
+  factor_kernel<<<dim3(num_frames, 2), kThreads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(a);
   return static_cast<int>(cudaGetLastError());
 }
