@@ -407,8 +407,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         mx.x = fmaxf(mx.x, v.x);
         mx.y = fmaxf(mx.y, v.y);
       }
+      // Lane l holds pixels 2l and 2l + 1.  In round it it stores the limbs of
+      // pixel 2l + (it ^ ((l >> 2) & 1)): the 32 rows of one store then fall
+      // on all eight 16-byte slots of the 128-byte swizzle (row & 7 takes
+      // every value), so each 16-byte store of the warp is four conflict-free
+      // wavefronts instead of eight.
+      const int hflip = (lane >> 2) & 1;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int it = 0; it < 2; ++it) {
+        const int h = it ^ hflip;
         const int pl = 2 * lane + h;
         const float m = h ? mx.y : mx.x;
         // 2^t with m 2^t in [2^21, 2^22): |q| <= 2^22, exact through the FMA rounding
@@ -420,7 +427,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int g = 0; g < 4; ++g) {
           int w[4];
 #pragma unroll
-          for (int e = 0; e < 4; ++e) w[e] = __float_as_int(fmaf(d[h][g * 4 + e], sc, kMagic)) - wbias;
+          for (int e = 0; e < 4; ++e) {
+            const float dv = h ? d[1][g * 4 + e] : d[0][g * 4 + e];
+            w[e] = __float_as_int(fmaf(dv, sc, kMagic)) - wbias;
+          }
           const uint32_t p01 = __byte_perm(w[0], w[1], 0x5140), p23 = __byte_perm(w[2], w[3], 0x5140);
           const uint32_t h01 = __byte_perm(w[0], w[1], 0x7362), h23 = __byte_perm(w[2], w[3], 0x7362);
           l2[g] = __byte_perm(p01, p23, 0x5410) ^ 0x80808080u;

@@ -22,6 +22,7 @@
 
 
 #include "launch_state.h"
+#include "sam_math.cuh"
 #include "tc.cuh"
 
 namespace hsi_b200 {
@@ -30,6 +31,10 @@ namespace {
 constexpr int kGroupThreads = 128;  // one consumer warpgroup
 constexpr int kPPT = 4;             // pixels per consumer thread
 constexpr int kTile = kGroupThreads * kPPT;
+// Both banks in one consumer group: two warpgroups, two pixels per thread
+// (twice the warps of one warpgroup at four pixels, for the same tile).
+constexpr int kFusedThreads = 256;
+constexpr int kFusedPPT = kTile / kFusedThreads;
 constexpr int kStageBands = 8;
 constexpr int kMaxTableFrames = 256;
 constexpr int kFiltersPerPass = HSI_MAX_FILTERS_PER_PASS;
@@ -92,6 +97,17 @@ __device__ __forceinline__ void load4<__half>(const __half* p, float v[4]) {
   v[1] = a.y;
   v[2] = b.x;
   v[3] = b.y;
+}
+
+template <typename T>
+__device__ __forceinline__ float2 load2(const T* p);
+template <>
+__device__ __forceinline__ float2 load2<float>(const float* p) {
+  return *reinterpret_cast<const float2*>(p);
+}
+template <>
+__device__ __forceinline__ float2 load2<__half>(const __half* p) {
+  return __half22float2(*reinterpret_cast<const __half2*>(p));
 }
 
 __device__ __forceinline__ void named_sync(int id, int threads) {
@@ -169,83 +185,73 @@ __device__ __forceinline__ void consume_stage(const T* stage, const float* filt2
   }
 }
 
-// Angle of a cosine clamped to [-1, 1] (a NaN clamps to -1, as with fminf/fmaxf).
-// arccos by Abramowitz & Stegun 4.4.46 (Hastings' approximation):
-//   acos(x) = sqrt(1 - x) (a0 + a1 x + ... + a7 x^7) + e(x),  |e| <= 2e-8 on [0, 1],
-// and acos(-x) = pi - acos(x).  In FP32 the result is within a few 1e-7 rad of
-// the exact angle, far inside the scorer's tolerances, at about half the
-// instructions of the library arccos; sqrt(y) is y rsqrt(y) (y = 0 gives 0).
-__device__ __forceinline__ float angle_of_cos(float c) {
-  c = fminf(fmaxf(c, -1.0f), 1.0f);
-  const float x = fabsf(c);
-  float p = -0.0012624911f;
-  p = fmaf(p, x, 0.0066700901f);
-  p = fmaf(p, x, -0.0170881256f);
-  p = fmaf(p, x, 0.0308918810f);
-  p = fmaf(p, x, -0.0501743046f);
-  p = fmaf(p, x, 0.0889789874f);
-  p = fmaf(p, x, -0.2145988016f);
-  p = fmaf(p, x, 1.5707963050f);
-  const float y = 1.0f - x;
-  const float r = y > 0.0f ? y * rsqrtf(y) * p : 0.0f;
-  return c < 0.0f ? 3.14159265358979f - r : r;
-}
-
-__device__ __forceinline__ void store4(float* dst, const float v[kPPT], int valid, bool vec) {
-  if (vec && valid == kPPT) {
-    *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+// A thread's PPT consecutive outputs: one vector store when all are valid and
+// `vec` (the address is PPT * 4-byte aligned), else element by element.
+template <int PPT>
+__device__ __forceinline__ void storev(float* dst, const float (&v)[PPT], int valid, bool vec) {
+  if (vec && valid == PPT) {
+    if constexpr (PPT == 4)
+      *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+    else
+      *reinterpret_cast<float2*>(dst) = make_float2(v[0], v[1]);
   } else {
 #pragma unroll
-    for (int j = 0; j < kPPT; ++j)
+    for (int j = 0; j < PPT; ++j)
       if (j < valid) dst[j] = v[j];
   }
 }
 
-__device__ __forceinline__ void store4i(int32_t* dst, const int32_t v[kPPT], int valid, bool vec) {
-  if (vec && valid == kPPT) {
-    *reinterpret_cast<int4*>(dst) = make_int4(v[0], v[1], v[2], v[3]);
+template <int PPT>
+__device__ __forceinline__ void storevi(int32_t* dst, const int32_t (&v)[PPT], int valid, bool vec) {
+  if (vec && valid == PPT) {
+    if constexpr (PPT == 4)
+      *reinterpret_cast<int4*>(dst) = make_int4(v[0], v[1], v[2], v[3]);
+    else
+      *reinterpret_cast<int2*>(dst) = make_int2(v[0], v[1]);
   } else {
 #pragma unroll
-    for (int j = 0; j < kPPT; ++j)
+    for (int j = 0; j < PPT; ++j)
       if (j < valid) dst[j] = v[j];
   }
 }
 
-__device__ __forceinline__ bool aligned16(const void* p) {
-  return (reinterpret_cast<uintptr_t>(p) & 15u) == 0;
+// Address aligned for a PPT-float vector store.
+template <int PPT>
+__device__ __forceinline__ bool aligned_v(const void* p) {
+  return (reinterpret_cast<uintptr_t>(p) & (PPT * 4 - 1)) == 0;
 }
 
-// SAM epilogue for one thread's 4 pixels starting at frame pixel p.
-template <int KG>
+// SAM epilogue for one thread's PPT pixels starting at frame pixel p.
+template <int KG, int PPT>
 __device__ void sam_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, int valid,
-                             const float (&acc)[KG][kPPT], const float (&nrm)[kPPT], const float* scale) {
+                             const float (&acc)[KG][PPT], const float (&nrm)[PPT], const float* scale) {
   {
     const bool first = pass == 0;
     const bool last = pass_count(F.num_sam, pass + 1) == 0;
     const int t0 = pass * kFiltersPerPass;
-    float rn[kPPT], best[kPPT];
-    int32_t best_t[kPPT];
+    float rn[PPT], best[PPT];
+    int32_t best_t[PPT];
 #pragma unroll
-    for (int j = 0; j < kPPT; ++j) {
+    for (int j = 0; j < PPT; ++j) {
       rn[j] = nrm[j] > 0.0f ? rsqrtf(nrm[j]) : 0.0f;
       best[j] = -2.0f;
       best_t[j] = -1;
     }
     if (!first) {
 #pragma unroll
-      for (int j = 0; j < kPPT; ++j) {
+      for (int j = 0; j < PPT; ++j) {
         if (j >= valid) continue;
         if (F.sam_best) best[j] = F.sam_best[p + j];
         if (F.sam_best_target) best_t[j] = F.sam_best_target[p + j];
       }
     }
-    const bool vec_maps = F.sam_maps && aligned16(F.sam_maps) && (F.map_stride & 3) == 0;
+    const bool vec_maps = F.sam_maps && aligned_v<PPT>(F.sam_maps) && (F.map_stride % PPT) == 0;
 #pragma unroll
     for (int k = 0; k < KG; ++k) {
       if (k < n_f) {
-        float c[kPPT];
+        float c[PPT];
 #pragma unroll
-        for (int j = 0; j < kPPT; ++j) {
+        for (int j = 0; j < PPT; ++j) {
           c[j] = acc[k][j] * rn[j] * scale[k];
           if (c[j] > best[j]) {
             best[j] = c[j];
@@ -253,62 +259,67 @@ __device__ void sam_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, i
           }
         }
         if (F.sam_maps) {
-          float a[kPPT];
+          float a[PPT];
 #pragma unroll
-          for (int j = 0; j < kPPT; ++j) a[j] = angle_of_cos(c[j]);
-          store4(F.sam_maps + static_cast<int64_t>(t0 + k) * F.map_stride + p, a, valid, vec_maps);
+          for (int j = 0; j < PPT; j += 2) {
+            const float2 v = angle_of_cos2(make_float2(c[j], c[j + 1]));
+            a[j] = v.x;
+            a[j + 1] = v.y;
+          }
+          storev<PPT>(F.sam_maps + static_cast<int64_t>(t0 + k) * F.map_stride + p, a, valid, vec_maps);
         }
       }
     }
     if (F.sam_best) {
-      float out[kPPT];
+      float out[PPT];
 #pragma unroll
-      for (int j = 0; j < kPPT; ++j) out[j] = last ? angle_of_cos(best[j]) : best[j];
-      store4(F.sam_best + p, out, valid, aligned16(F.sam_best));
+      for (int j = 0; j < PPT; ++j) out[j] = last ? angle_of_cos(best[j]) : best[j];
+      storev<PPT>(F.sam_best + p, out, valid, aligned_v<PPT>(F.sam_best));
     }
-    if (F.sam_best_target) store4i(F.sam_best_target + p, best_t, valid, aligned16(F.sam_best_target));
+    if (F.sam_best_target) storevi<PPT>(F.sam_best_target + p, best_t, valid, aligned_v<PPT>(F.sam_best_target));
   }
 }
 
-template <int KG>
+template <int KG, int PPT>
 __device__ void cem_epilogue(const hsi_frame& F, int pass, int n_f, int64_t p, int valid,
-                             const float (&acc)[KG][kPPT]) {
+                             const float (&acc)[KG][PPT]) {
   {
     const bool first = pass == 0;
     const int t0 = pass * kFiltersPerPass;
-    float best[kPPT];
-    int32_t best_t[kPPT];
+    float best[PPT];
+    int32_t best_t[PPT];
 #pragma unroll
-    for (int j = 0; j < kPPT; ++j) {
+    for (int j = 0; j < PPT; ++j) {
       best[j] = -INFINITY;
       best_t[j] = -1;
     }
     if (!first) {
 #pragma unroll
-      for (int j = 0; j < kPPT; ++j) {
+      for (int j = 0; j < PPT; ++j) {
         if (j >= valid) continue;
         if (F.cem_best) best[j] = F.cem_best[p + j];
         if (F.cem_best_target) best_t[j] = F.cem_best_target[p + j];
       }
     }
-    const bool vec_maps = F.cem_maps && aligned16(F.cem_maps) && (F.map_stride & 3) == 0;
+    const bool vec_maps = F.cem_maps && aligned_v<PPT>(F.cem_maps) && (F.map_stride % PPT) == 0;
 #pragma unroll
     for (int k = 0; k < KG; ++k) {
       if (k < n_f) {
-        float r[kPPT];
+        float r[PPT];
 #pragma unroll
-        for (int j = 0; j < kPPT; ++j) {
+        for (int j = 0; j < PPT; ++j) {
           r[j] = acc[k][j];
           if (r[j] > best[j]) {
             best[j] = r[j];
             best_t[j] = t0 + k;
           }
         }
-        if (F.cem_maps) store4(F.cem_maps + static_cast<int64_t>(t0 + k) * F.map_stride + p, r, valid, vec_maps);
+        if (F.cem_maps)
+          storev<PPT>(F.cem_maps + static_cast<int64_t>(t0 + k) * F.map_stride + p, r, valid, vec_maps);
       }
     }
-    if (F.cem_best) store4(F.cem_best + p, best, valid, aligned16(F.cem_best));
-    if (F.cem_best_target) store4i(F.cem_best_target + p, best_t, valid, aligned16(F.cem_best_target));
+    if (F.cem_best) storev<PPT>(F.cem_best + p, best, valid, aligned_v<PPT>(F.cem_best));
+    if (F.cem_best_target) storevi<PPT>(F.cem_best_target + p, best_t, valid, aligned_v<PPT>(F.cem_best_target));
   }
 }
 
@@ -388,43 +399,41 @@ __device__ __forceinline__ void consumer_loop(const ScoreParams& prm, const int*
         }
         if constexpr (kSam) {
           const float n[kPPT] = {nrm[0].x, nrm[0].y, nrm[1].x, nrm[1].y};
-          sam_epilogue<KG>(F, prm.pass, n_f, p, valid, a, n, scale);
+          sam_epilogue<KG, kPPT>(F, prm.pass, n_f, p, valid, a, n, scale);
         } else {
-          cem_epilogue<KG>(F, prm.pass, n_f, p, valid, a);
+          cem_epilogue<KG, kPPT>(F, prm.pass, n_f, p, valid, a);
         }
       }
     }
   }
 }
 
-// Fused consumer: one warpgroup scores the SAM and the CEM bank together, so
+// Fused consumer: two warpgroups score the SAM and the CEM bank together, so
 // each pixel leaves shared memory once for all KS + KC filters.  The bank is
 // stored band-major without duplication, [b][KS SAM | KC CEM]; accumulators
 // are filter pairs per pixel, (acc_k, acc_k+1) += (x, x) * (f_k, f_k+1), the
-// pixel duplicated in a register pair for the packed FMA.
+// pixel duplicated in a register pair for the packed FMA.  Two pixels per
+// thread keep the accumulators at 2 * (KS + KC) registers, so 256 consumer
+// threads fit per CTA at three CTAs per SM (twice the warps of one warpgroup
+// at four pixels per thread, to hide the shared-memory and FMA latencies).
 template <typename T, int K>
 __device__ __forceinline__ void consume_stage_fused(const T* stage, const float* filt, int nb, int tid,
-                                                    float2 (&acc)[K / 2][kPPT], float2 (&nrm)[2]) {
-  const T* src = stage + tid * kPPT;
+                                                    float2 (&acc)[K / 2][kFusedPPT], float2& nrm) {
+  static_assert(kFusedPPT == 2, "two pixels per fused consumer thread");
+  const T* src = stage + tid * kFusedPPT;
   auto band = [&](int i) {
-    float v[kPPT];
-    load4<T>(src + i * kTile, v);
-    const float2 v01 = make_float2(v[0], v[1]), v23 = make_float2(v[2], v[3]);
-    nrm[0] = ffma2(v01, v01, nrm[0]);
-    nrm[1] = ffma2(v23, v23, nrm[1]);
-    float2 d[kPPT];
-#pragma unroll
-    for (int j = 0; j < kPPT; ++j) d[j] = make_float2(v[j], v[j]);
+    const float2 v = load2<T>(src + i * kTile);
+    nrm = ffma2(v, v, nrm);
+    const float2 d0 = make_float2(v.x, v.x), d1 = make_float2(v.y, v.y);
     const float* fr = filt + i * K;
 #pragma unroll
     for (int k = 0; k < K; k += 4) {
       const float4 f = ld_shared_f4(fr + k);  // (f_k, f_k+1, f_k+2, f_k+3)
       const float2 fa = make_float2(f.x, f.y), fb = make_float2(f.z, f.w);
-#pragma unroll
-      for (int j = 0; j < kPPT; ++j) {
-        acc[k / 2][j] = ffma2(d[j], fa, acc[k / 2][j]);
-        acc[k / 2 + 1][j] = ffma2(d[j], fb, acc[k / 2 + 1][j]);
-      }
+      acc[k / 2][0] = ffma2(d0, fa, acc[k / 2][0]);
+      acc[k / 2][1] = ffma2(d1, fa, acc[k / 2][1]);
+      acc[k / 2 + 1][0] = ffma2(d0, fb, acc[k / 2 + 1][0]);
+      acc[k / 2 + 1][1] = ffma2(d1, fb, acc[k / 2 + 1][1]);
     }
   };
   if (nb == kStageBands) {
@@ -441,6 +450,7 @@ __device__ __forceinline__ void consumer_loop_fused(const ScoreParams& prm, cons
                                                     uint64_t* empty, volatile int* abort_flag, float* filt,
                                                     float* scale, int tid, int lane) {
   constexpr int K = KS + KC;
+  constexpr int PPT = kFusedPPT;
   const int nframes = prm.num_frames;
   int cur_frame = -1;
   int n_s = 0, n_c = 0;
@@ -452,11 +462,11 @@ __device__ __forceinline__ void consumer_loop_fused(const ScoreParams& prm, cons
     const hsi_frame& F = frame_at(prm, f);
     const int B = F.bands;
     if (f != cur_frame) {
-      named_sync(1, kGroupThreads);
+      named_sync(1, kFusedThreads);
       n_s = pass_count(F.num_sam, prm.pass);
       n_c = pass_count(F.num_cem, prm.pass);
       const int t0 = prm.pass * kFiltersPerPass;
-      for (int i = tid; i < B * K; i += kGroupThreads) {
+      for (int i = tid; i < B * K; i += kFusedThreads) {
         const int b = i / K, k = i % K;
         float v = 0.0f;
         if (k < KS) {
@@ -470,19 +480,19 @@ __device__ __forceinline__ void consumer_loop_fused(const ScoreParams& prm, cons
         const float nrm = tid < n_s ? F.sam_norms[t0 + tid] : 0.0f;
         scale[tid] = nrm > 0.0f ? 1.0f / nrm : 0.0f;
       }
-      named_sync(1, kGroupThreads);
+      named_sync(1, kFusedThreads);
       cur_frame = f;
     }
     const int64_t P = static_cast<int64_t>(F.height) * F.width;
     const int64_t p0 = static_cast<int64_t>(tile - prefix[f]) * kTile;
     const bool active = n_s > 0 || n_c > 0;
 
-    float2 acc[K / 2][kPPT];
-    float2 nrm[2] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+    float2 acc[K / 2][PPT];
+    float2 nrm = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int k = 0; k < K / 2; ++k)
 #pragma unroll
-      for (int j = 0; j < kPPT; ++j) acc[k][j] = make_float2(0.0f, 0.0f);
+      for (int j = 0; j < PPT; ++j) acc[k][j] = make_float2(0.0f, 0.0f);
 
     for (int b0 = 0; b0 < B; b0 += kStageBands) {
       const int nb = B - b0 < kStageBands ? B - b0 : kStageBands;
@@ -502,27 +512,27 @@ __device__ __forceinline__ void consumer_loop_fused(const ScoreParams& prm, cons
       ++it;
     }
     if (active && !aborted) {
-      const int64_t p = p0 + tid * kPPT;
+      const int64_t p = p0 + tid * PPT;
       const int64_t rem = P - p;
-      const int valid = rem <= 0 ? 0 : (rem >= kPPT ? kPPT : static_cast<int>(rem));
+      const int valid = rem <= 0 ? 0 : (rem >= PPT ? PPT : static_cast<int>(rem));
       if (valid > 0) {
         if (n_s > 0) {
-          float a[KS][kPPT];
+          float a[KS][PPT];
 #pragma unroll
           for (int k = 0; k < KS; ++k)
 #pragma unroll
-            for (int j = 0; j < kPPT; ++j) a[k][j] = (k & 1) ? acc[k / 2][j].y : acc[k / 2][j].x;
-          const float n[kPPT] = {nrm[0].x, nrm[0].y, nrm[1].x, nrm[1].y};
-          sam_epilogue<KS>(F, prm.pass, n_s, p, valid, a, n, scale);
+            for (int j = 0; j < PPT; ++j) a[k][j] = (k & 1) ? acc[k / 2][j].y : acc[k / 2][j].x;
+          const float n[PPT] = {nrm.x, nrm.y};
+          sam_epilogue<KS, PPT>(F, prm.pass, n_s, p, valid, a, n, scale);
         }
         if (n_c > 0) {
-          float a[KC][kPPT];
+          float a[KC][PPT];
 #pragma unroll
           for (int k = 0; k < KC; ++k)
 #pragma unroll
-            for (int j = 0; j < kPPT; ++j)
+            for (int j = 0; j < PPT; ++j)
               a[k][j] = ((KS + k) & 1) ? acc[(KS + k) / 2][j].y : acc[(KS + k) / 2][j].x;
-          cem_epilogue<KC>(F, prm.pass, n_c, p, valid, a);
+          cem_epilogue<KC, PPT>(F, prm.pass, n_c, p, valid, a);
         }
       }
     }
@@ -536,11 +546,15 @@ constexpr bool fused_banks() {
 }
 
 // Kernel: KS SAM filters and KC CEM filters per pass (0 = that warpgroup is
-// absent; both in one warpgroup when fused_banks).  Block = (groups * 128 +
-// 32) threads; the last warp produces.
+// absent; both in one consumer group of kFusedThreads when fused_banks).
+// Block = consumer threads + 32; the last warp produces.
 template <int KS, int KC>
 constexpr int score_groups() {
   return fused_banks<KS, KC>() ? 1 : (KS > 0) + (KC > 0);
+}
+template <int KS, int KC>
+constexpr int consumer_threads() {
+  return fused_banks<KS, KC>() ? kFusedThreads : score_groups<KS, KC>() * kGroupThreads;
 }
 // Filter slots per band per group in shared memory (duplicated pairs in the
 // two-group layout, plain in the fused one).
@@ -555,7 +569,7 @@ constexpr int score_stages() {
 }
 
 template <typename T, int KS, int KC>
-__global__ void __launch_bounds__(score_groups<KS, KC>() * kGroupThreads + 32, fused_banks<KS, KC>() ? 3 : 1)
+__global__ void __launch_bounds__(consumer_threads<KS, KC>() + 32, fused_banks<KS, KC>() ? 3 : 1)
     score_kernel(const __grid_constant__ ScoreParams prm, int max_bands) {
   constexpr int kGroups = score_groups<KS, KC>();
   constexpr int kStages = score_stages<T, KS, KC>();
@@ -586,7 +600,7 @@ __global__ void __launch_bounds__(score_groups<KS, KC>() * kGroupThreads + 32, f
     *abort_flag = 0;
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kGroups * (kGroupThreads / 32));
+      mbar_init(&empty[s], consumer_threads<KS, KC>() / 32);
     }
     fence_barrier_init();
   }
@@ -600,7 +614,7 @@ __global__ void __launch_bounds__(score_groups<KS, KC>() * kGroupThreads + 32, f
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
 
-  if (warp == kGroups * (kGroupThreads / 32)) {
+  if (warp == consumer_threads<KS, KC>() / 32) {
     // ---------------- producer warp ----------------
     if (lane == 0) {
       uint32_t it = 0;
@@ -644,15 +658,17 @@ __global__ void __launch_bounds__(score_groups<KS, KC>() * kGroupThreads + 32, f
   }
 
   // ---------------- consumer warpgroups ----------------
+  if constexpr (fused_banks<KS, KC>()) {
+    float* filt = reinterpret_cast<float*>(smem + L.filt_off);
+    float* scale = reinterpret_cast<float*>(smem + L.scale_off);
+    consumer_loop_fused<T, KS, KC, kStages>(prm, prefix, total_tiles, smem, L.stage_bytes, full, empty, abort_flag,
+                                            filt, scale, threadIdx.x, lane);
+    return;
+  }
   const int group = warp / (kGroupThreads / 32);  // 0: SAM if KS > 0, else CEM; 1: CEM
   const int tid = threadIdx.x - group * kGroupThreads;
   float* filt = reinterpret_cast<float*>(smem + L.filt_off) + static_cast<size_t>(group) * max_bands * kSlots;
   float* scale = reinterpret_cast<float*>(smem + L.scale_off) + group * kFiltersPerPass;
-  if constexpr (fused_banks<KS, KC>()) {
-    consumer_loop_fused<T, KS, KC, kStages>(prm, prefix, total_tiles, smem, L.stage_bytes, full, empty, abort_flag,
-                                            filt, scale, tid, lane);
-    return;
-  }
   if constexpr (KS > 0) {
     if (group == 0) {
       consumer_loop<T, KS, true, kStages>(prm, prefix, total_tiles, smem, L.stage_bytes, full, empty,
@@ -1172,7 +1188,7 @@ template <typename T, int KS, int KC>
 int launch_instance(const ScoreParams& p, int max_bands, int ctas_per_sm, cudaStream_t stream) {
   constexpr int kGroups = score_groups<KS, KC>();
   const SmemLayout L = smem_layout<T>(kGroups, max_bands, score_slots<KS, KC>(), score_stages<T, KS, KC>());
-  const int threads = kGroups * kGroupThreads + 32;
+  const int threads = consumer_threads<KS, KC>() + 32;
   auto kernel = score_kernel<T, KS, KC>;
   // The layout follows the band count of the call.  The device's limit for
   // this kernel only ever rises, so a concurrent call with fewer bands cannot
