@@ -78,21 +78,15 @@ cudaError_t launch_sam_best(SamVariant variant, const void* d_cube, CubeShape sh
   if (!d_cube || !shape.valid() || !d_targets || !d_target_norms || num_targets <= 0 || !d_score)
     return cudaErrorInvalidValue;
   const std::size_t stride = bsq_plane_stride(shape);
-  const void* cube = d_cube;
-  void* scratch = nullptr;
   int dtype = HSI_F32;
   if (variant == SamVariant::Half) {
     dtype = HSI_F16;
   } else if (variant == SamVariant::BipDirect) {
-    const cudaError_t e = detail::stream_scratch(stream, stride * shape.bands * sizeof(float), &scratch);
-    if (e != cudaSuccess) return e;
-    const int st = hsi_transpose_bip_to_bsq(static_cast<const float*>(d_cube), static_cast<float*>(scratch),
-                                            shape.height, shape.width, shape.bands,
-                                            static_cast<int64_t>(stride), as_stream(stream));
-    if (st != HSI_OK) return to_cuda(st);
-    cube = scratch;
+    // one pass over the BIP cube, the transpose fused into the scorer
+    return to_cuda(hsi_sam_bip(static_cast<const float*>(d_cube), shape.height, shape.width, shape.bands, d_targets,
+                               d_target_norms, num_targets, nullptr, 0, d_score, d_target_id, as_stream(stream)));
   }
-  hsi_frame f = frame_of(cube, shape, dtype, stride);
+  hsi_frame f = frame_of(d_cube, shape, dtype, stride);
   f.sam_targets = d_targets;
   f.sam_norms = d_target_norms;
   f.num_sam = num_targets;

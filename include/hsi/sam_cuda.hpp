@@ -16,9 +16,8 @@
 namespace hsi {
 
 // reference include/hsi/sam_cuda.hpp:18-36.  Baseline and Optimized score an
-// fp32 BSQ cube, Half an fp16 BSQ cube, BipDirect an fp32 BIP cube (it is
-// transposed on the device into the stream's scratch first; see
-// release_launch_workspaces).
+// fp32 BSQ cube, Half an fp16 BSQ cube, BipDirect an fp32 BIP cube (packed,
+// in one pass: the transpose is fused into the scorer, hsi_sam_bip).
 enum class SamVariant {
   Baseline,
   Optimized,
@@ -66,8 +65,7 @@ cudaError_t launch_transpose_bip_to_bsq(const float* d_src, float* d_dst, CubeSh
 cudaError_t launch_narrow_to_half(const float* d_src, void* d_dst, std::size_t count, cudaStream_t stream);
 
 // Scratch of the launchers whose reference signatures take no workspace
-// (launch_detect, launch_sam_best with BipDirect, the moment accumulators,
-// launch_rx_ace).  No counterpart in the reference.  Each (device, stream)
+// (launch_detect, the moment accumulators, launch_rx_ace).  No counterpart in the reference.  Each (device, stream)
 // keeps one device buffer between calls, grown only when a call needs more
 // than earlier calls on that stream did: steady-state calls allocate nothing,
 // and a graph may capture them once one call at the largest size has run

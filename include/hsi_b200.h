@@ -399,6 +399,19 @@ HSI_API int hsi_narrow_to_half(const float* d_src, void* d_dst, int64_t count, h
 HSI_API int hsi_transpose_bip_to_bsq(const float* d_src, float* d_dst, int height, int width, int bands,
                                      int64_t plane_stride, hsi_stream_t stream);
 
+/* SAM of a BIP cube (pixel-major: `bands` floats per pixel, packed, 4-byte
+ * aligned) in one pass, without a BSQ copy: the transpose is fused into the
+ * scoring kernel.  Outputs as hsi_score_frames' SAM outputs (each nullable,
+ * at least one given): d_maps (num_targets maps at map_stride), d_best (the
+ * smallest angle), d_best_target (its index, lowest on ties); angles are
+ * bit-identical to scoring the same cube in BSQ.  All 1..64 targets are
+ * scored in one pass.  Replaces the reference's direct BIP scorer behind
+ * launch_sam_best(SamVariant::BipDirect) (include/hsi/sam_cuda.hpp:91-96,
+ * src/sam.cu:80-125,391-398). */
+HSI_API int hsi_sam_bip(const float* d_cube, int height, int width, int bands, const float* d_targets,
+                        const float* d_target_norms, int num_targets, float* d_maps, int64_t map_stride,
+                        float* d_best, int32_t* d_best_target, hsi_stream_t stream);
+
 /* Snapshot-mosaic demosaic on the device: raw frame (raw_height x raw_width
  * floats, row-major) -> BSQ cube of (raw_height/period) x (raw_width/period)
  * pixels and `bands` <= period^2 bands, element type `dtype`.  Band b takes
