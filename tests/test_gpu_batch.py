@@ -5,14 +5,19 @@ mosaic demosaiced inside the run.
 Checked: the CUDA-graph replay reproduces the eager run bit for bit; each
 frame's SAM map matches the FP64 oracle (the scorer's tolerances: 1e-4 rad
 away from zero angle, 2e-3 rad near it, where acos amplifies the FP32
-cosine's rounding), its RX / ACE maps match
-the single-frame path on the same statistics within the RX / ACE tolerance
-(RX 1e-4 relative, ACE 1e-4 absolute: the autotuner may pick either RX path),
-and its detection lists equal hsi_detect run on the batch's own maps.
+cosine's rounding); its RX / ACE maps match the FP64 oracle on the frame's
+own FP64 statistics (RX 1e-4 relative, ACE 1e-4 absolute, whichever RX path
+the autotuner picked); and its SAM, ACE and RX lists equal the oracle's
+detect on the oracle's maps under the detection-set parity rule of
+tests/parity.py (SAM 2e-3 rad -- the scorer's bound near zero angle --,
+ACE 1e-4, RX 1e-4 of the value).
 """
 import numpy as np
 import pytest
 import torch
+
+import oracle
+import parity
 
 pytestmark = pytest.mark.gpu
 
@@ -60,7 +65,7 @@ def _collect(hsi, batch, hosts):
     return out
 
 
-def test_batch_eager_graph_and_single_frame_agree(hsi, orc):
+def test_batch_eager_graph_and_oracle_agree(hsi, orc):
     frames, hosts = _frames(hsi)
     batch = hsi.Batch(frames, sam_threshold=0.12, capacity=2048, autotune=True)
     stream = torch.cuda.Stream()
@@ -82,30 +87,30 @@ def test_batch_eager_graph_and_single_frame_agree(hsi, orc):
         P = h * w
         host = cube[:, :P].float().cpu().numpy()
         # SAM against the FP64 oracle
-        want, _ = orc.sam_best(host, targets)
+        want, which_sam = orc.sam_best(host, targets)
         err = np.abs(e["sam_best"].cpu().numpy() - want)
         assert err.max() <= 2e-3 and err[want > 0.05].max() <= 1e-4
-        # RX / ACE against the single-frame path on the same statistics
-        gm = hsi.scene_moments(cube, h, w, b, dtype=dt)
-        s64, _, st = hsi.build_statistics(gm, b, torch.from_numpy(targets).cuda(), loading=1e-6)
-        rx = torch.zeros(P, device="cuda")
-        ace = torch.zeros(P, device="cuda")
-        hsi.rx_ace(cube, h, w, b, s64[0], targets.shape[0], dtype=dt, rx=rx, ace_best=ace, simt=b > 127)
-        torch.cuda.synchronize()
-        r0 = rx.cpu().numpy()
-        assert np.max(np.abs(e["rx"].cpu().numpy() - r0) / np.maximum(1.0, np.abs(r0))) <= 1e-4
-        assert np.max(np.abs(e["ace_best"].cpu().numpy() - ace.cpu().numpy())) <= 1e-4
-        # lists: hsi_detect on the batch's own maps
-        maps = [(e["sam_best"], e["sam_target"], 0.12, hsi.LOWER_IS_BETTER),
-                (e["ace_best"], e["ace_target"], 0.5, hsi.HIGHER_IS_BETTER),
-                (e["rx"], None, e["rx_threshold"], hsi.HIGHER_IS_BETTER)]
-        for k, (score, tgt, thr, pol) in enumerate(maps):
-            count, lst = hsi.detect(score, tgt, h, w, thr, 2, pol, 2048)
-            torch.cuda.synchronize()
-            n = int(count.item())
-            assert n == int(e["counts"][k].item()), (i, k)
-            m = min(n, 2048)
-            assert torch.equal(lst[:m], e["lists"][k][:m]), (i, k)
+        # RX / ACE against the FP64 oracle on the frame's FP64 statistics
+        st, S = orc.build_statistics(*orc.moments(host), targets, 1e-6)
+        assert st == 0
+        best0, which0, rx0, all0 = orc.ace(host, S)
+        rx_g = e["rx"].cpu().numpy()
+        assert np.max(np.abs(rx_g - rx0) / np.maximum(1.0, np.abs(rx0))) <= 1e-4
+        assert np.max(np.abs(e["ace_best"].cpu().numpy() - best0)) <= 1e-4
+        # lists against the oracle's detect on the oracle's maps
+        sam_all = orc.sam_all(host, targets)
+        oracle_maps = [(want, which_sam, 0.12, False, 2e-3, parity.best_margin(sam_all, False), False),
+                       (best0, which0, 0.5, True, 1e-4, parity.best_margin(all0, True), False),
+                       (rx0, None, float(e["rx_threshold"]), True, 1e-4, None, True)]
+        for k, (score, which, thr, higher, tol, margin, rel) in enumerate(oracle_maps):
+            n = int(e["counts"][k].item())
+            assert n <= 2048, (i, k)
+            lst = e["lists"][k][:n].cpu().numpy()
+            got = np.zeros(n, oracle.DETECTION_DTYPE)
+            got["x"], got["y"], got["target"] = lst[:, 0], lst[:, 1], lst[:, 2]
+            got["score"] = lst[:, 3].view(np.float32)
+            _, ref = orc.detect(score, which, h, w, thr, 2, higher)
+            parity.compare_lists(got, ref, score, h, w, thr, 2, tol, margin=margin, rel=rel)
     batch.close()
 
 
