@@ -5,15 +5,19 @@
 // (src/sam.cu:281-309).  Here the transpose is fused into the scoring pass:
 // the cube crosses HBM once, and no BSQ scratch copy exists.
 //
-// Each warp takes tiles of 32 pixels.  A tile's 32 * B floats are contiguous
-// in BIP, so the warp reads them with coalesced 16-byte loads and scatters
-// them into a per-warp shared-memory buffer laid out band-major with a row
-// stride of 33 floats (bank-conflict free both ways).  Then lane p scores
-// pixel p: its squared norm and its dot product with every target, in band
-// order with one fmaf per band -- the same operations in the same order as
-// the BSQ scorer (score.cu), so the angles, best angles and best targets are
-// bit-identical to scoring the transposed cube.  All targets are scored from
-// shared memory in one pass over HBM (groups of 16 accumulators).
+// Each warp takes tiles of 32 pixels on its own, as a two-step software
+// pipeline.  A tile's 32 * B floats are contiguous in BIP: the warp copies
+// them into a raw shared-memory buffer with 16-byte cp.async copies, then
+// transposes them into a band-major buffer in which pixel p of band b sits in
+// column p ^ (b / 4) mod 32 (both the transposing stores and the per-band
+// reads are free of bank conflicts), then starts the next tile's copies into
+// the raw buffer and scores this tile from the band-major one meanwhile.
+// Lane p scores pixel p: its squared norm and its dot product with every
+// target, in band order with one fmaf per band and target -- the same
+// operations in the same order as the BSQ scorer (score.cu), so the angles,
+// best angles and best targets are bit-identical to scoring the transposed
+// cube.  All targets are scored from shared memory in one pass over HBM
+// (groups of 16, two targets per packed FMA).
 #include "common.cuh"
 #include "launch_state.h"
 #include "sam_math.cuh"
@@ -21,9 +25,8 @@
 namespace hsi_b200 {
 namespace {
 
-constexpr int kWarps = 4;              // warps per block
+constexpr int kWarps = 1;              // warps per block: each warp runs its own pipeline
 constexpr int kPx = 32;                // pixels per warp tile
-constexpr int kStride = kPx + 1;       // floats between band rows of the tile buffer
 constexpr int kGroup = 16;             // targets per accumulator group
 constexpr int kMaxTargets = 64;
 
@@ -39,18 +42,46 @@ struct BipArgs {
   int32_t* best_t;     // nullable
 };
 
+// floats of one warp's tile buffer: 32 pixels x bands, rounded up to 4
+__host__ __device__ inline int tile_floats(int bands) { return (kPx * bands + 3) & ~3; }
+
+// floats of the target bank, rounded up to 4 so that the tile buffers after
+// it start on 16 bytes
+__host__ __device__ inline int bank_floats(int bands, int targets) { return (bands * targets + 3) & ~3; }
+
 __host__ __device__ inline size_t bip_smem_bytes(int bands, int targets) {
-  return sizeof(float) * (static_cast<size_t>(bands) * targets + kMaxTargets +
-                          static_cast<size_t>(kWarps) * bands * kStride);
+  return sizeof(float) * (static_cast<size_t>(bank_floats(bands, targets)) + kMaxTargets +
+                          static_cast<size_t>(kWarps) * 2 * tile_floats(bands));
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Column of pixel p in band row b of the band-major buffer.
+__device__ __forceinline__ int tcol(int b, int p) { return p ^ ((b >> 2) & 31); }
+
+// Start copying the tile at p0 (npx pixels) into raw: 16-byte cp.async copies
+// when the tile's start is 16-byte aligned, plain loads for the rest; the
+// buffer is zero-filled to a multiple of four floats.
+__device__ __forceinline__ void load_tile(float* raw, const float* src, int n, int lane, bool aligned) {
+  const int n4 = aligned ? n / 4 : 0;
+  for (int i = lane; i < n4; i += 32) cp_async16(raw + 4 * i, src + 4 * i);
+  cp_async_commit();
+  for (int e = 4 * n4 + lane; e < ((n + 3) & ~3); e += 32) raw[e] = e < n ? __ldg(src + e) : 0.0f;
 }
 
 __global__ void __launch_bounds__(kWarps * 32) sam_bip_kernel(const BipArgs a) {
-  extern __shared__ float sm[];
+  extern __shared__ __align__(16) float sm[];
   const int B = a.bands, T = a.targets;
-  float* tg = sm;                 // [b][t]
-  float* scale = tg + B * T;      // [t] = 1 / |r_t| (0 for a zero target)
+  float* tg = sm;                              // [b][t]
+  float* scale = tg + bank_floats(B, T);       // [t] = 1 / |r_t| (0 for a zero target)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* buf = scale + kMaxTargets + static_cast<size_t>(warp) * B * kStride;
+  const int tf = tile_floats(B);
+  float* raw = scale + kMaxTargets + static_cast<size_t>(warp) * 2 * tf;  // [p][b] as copied, 16-byte aligned
+  float* tb = raw + tf;                                                     // [b][tcol(b, p)]
   for (int i = threadIdx.x; i < B * T; i += blockDim.x) {
     const int b = i / T, t = i % T;
     tg[i] = a.lib[static_cast<int64_t>(t) * B + b];
@@ -59,52 +90,60 @@ __global__ void __launch_bounds__(kWarps * 32) sam_bip_kernel(const BipArgs a) {
   __syncthreads();
 
   const int64_t ntiles = div_up<int64_t>(a.pixels, kPx);
-  // 128 floats (32 lanes x one float4) advance a lane by this many pixels and bands
+  const int64_t step = static_cast<int64_t>(gridDim.x) * kWarps;
+  const bool base_aligned = (reinterpret_cast<uintptr_t>(a.cube) & 15u) == 0;
+  // a float4 of the raw tile advances a lane's (pixel, band) by 128 floats per round
   const int step_p = 128 / B, step_b = 128 % B;
-  for (int64_t tile = static_cast<int64_t>(blockIdx.x) * kWarps + warp; tile < ntiles;
-       tile += static_cast<int64_t>(gridDim.x) * kWarps) {
+  int64_t tile = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
+  if (tile < ntiles) {
     const int64_t p0 = tile * kPx;
     const int npx = static_cast<int>(a.pixels - p0 < kPx ? a.pixels - p0 : kPx);
-    const float* src = a.cube + p0 * B;
+    load_tile(raw, a.cube + p0 * B, npx * B, lane, base_aligned);
+  }
+  for (; tile < ntiles; tile += step) {
+    const int64_t p0 = tile * kPx;
+    const int npx = static_cast<int>(a.pixels - p0 < kPx ? a.pixels - p0 : kPx);
     const int n = npx * B;
-    // ---- load and transpose: element e = p B + b goes to buf[b * kStride + p]
-    if (npx == kPx && B >= 4 && (reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
-      const float4* s4 = reinterpret_cast<const float4*>(src);
+    cp_async_wait_all();
+    __syncwarp();
+    // ---- transpose raw [p][b] -> tb [b][tcol(b, p)], one float4 of raw per lane and round
+    {
       int e = 4 * lane;
       int p = e / B, b = e - p * B;
-#pragma unroll 4
-      for (int i = lane; i < n / 4; i += 32) {
-        const float4 v = __ldg(s4 + i);
+      for (int i = lane; 4 * i < n; i += 32) {
+        const float4 v = *reinterpret_cast<const float4*>(raw + 4 * i);
         const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           int bb = b + k, pp = p;
-          if (bb >= B) {
+          while (bb >= B) {
             bb -= B;
             ++pp;
           }
-          buf[bb * kStride + pp] = vv[k];
+          if (pp < npx) tb[bb * kPx + tcol(bb, pp)] = vv[k];
         }
         b += step_b;
         p += step_p;
-        if (b >= B) {
+        while (b >= B) {
           b -= B;
           ++p;
         }
       }
-    } else {
-      for (int e = lane; e < n; e += 32) {
-        const int p = e / B, b = e - p * B;
-        buf[b * kStride + p] = __ldg(src + e);
-      }
     }
     __syncwarp();
+    // ---- the next tile's copies run while this one is scored
+    const int64_t next = tile + step;
+    if (next < ntiles) {
+      const int64_t q0 = next * kPx;
+      const int nq = static_cast<int>(a.pixels - q0 < kPx ? a.pixels - q0 : kPx);
+      load_tile(raw, a.cube + q0 * B, nq * B, lane, base_aligned);
+    }
     // ---- score: lane = pixel
     if (lane < npx) {
       const int64_t px = p0 + lane;
       float nrm = 0.0f;
       for (int b = 0; b < B; ++b) {
-        const float x = buf[b * kStride + lane];
+        const float x = tb[b * kPx + tcol(b, lane)];
         nrm = fmaf(x, x, nrm);
       }
       const float rn = nrm > 0.0f ? rsqrtf(nrm) : 0.0f;
@@ -112,21 +151,36 @@ __global__ void __launch_bounds__(kWarps * 32) sam_bip_kernel(const BipArgs a) {
       int32_t best_t = -1;
       for (int t0 = 0; t0 < T; t0 += kGroup) {
         const int nt = T - t0 < kGroup ? T - t0 : kGroup;
-        float acc[kGroup];
+        float2 acc[kGroup / 2];
 #pragma unroll
-        for (int k = 0; k < kGroup; ++k) acc[k] = 0.0f;
-        for (int b = 0; b < B; ++b) {
-          const float x = buf[b * kStride + lane];
-          const float* tr = tg + b * T + t0;
+        for (int k = 0; k < kGroup / 2; ++k) acc[k] = make_float2(0.0f, 0.0f);
+        if (nt == kGroup && (T & 1) == 0) {
+          for (int b = 0; b < B; ++b) {
+            const float x = tb[b * kPx + tcol(b, lane)];
+            const float2 d = make_float2(x, x);
+            const float2* tr = reinterpret_cast<const float2*>(tg + b * T + t0);
 #pragma unroll
-          for (int k = 0; k < kGroup; ++k)
-            if (k < nt) acc[k] = fmaf(x, tr[k], acc[k]);
+            for (int k = 0; k < kGroup / 2; ++k) acc[k] = ffma2(d, tr[k], acc[k]);
+          }
+        } else {
+          for (int b = 0; b < B; ++b) {
+            const float x = tb[b * kPx + tcol(b, lane)];
+            const float* tr = tg + b * T + t0;
+#pragma unroll
+            for (int k = 0; k < kGroup; ++k)
+              if (k < nt) {
+                if (k & 1)
+                  acc[k / 2].y = fmaf(x, tr[k], acc[k / 2].y);
+                else
+                  acc[k / 2].x = fmaf(x, tr[k], acc[k / 2].x);
+              }
+          }
         }
 #pragma unroll
         for (int k = 0; k < kGroup; k += 2) {
           if (k >= nt) break;
-          const float c0 = acc[k] * rn * scale[t0 + k];
-          const float c1 = k + 1 < nt ? acc[k + 1] * rn * scale[t0 + k + 1] : -2.0f;
+          const float c0 = acc[k / 2].x * rn * scale[t0 + k];
+          const float c1 = k + 1 < nt ? acc[k / 2].y * rn * scale[t0 + k + 1] : -2.0f;
           if (c0 > best) {
             best = c0;
             best_t = t0 + k;
@@ -147,6 +201,7 @@ __global__ void __launch_bounds__(kWarps * 32) sam_bip_kernel(const BipArgs a) {
     }
     __syncwarp();
   }
+  cp_async_wait_all();  // never leave copies in flight into shared memory
 }
 
 }  // namespace
