@@ -109,8 +109,8 @@ __device__ void diag_block(double* A, double* W, double* vs, int k0, int kb, int
     if (k < kb) {
       const double akk = __shfl_sync(kAll, a[k], k);
       ok = ok && akk > 0.0;
-      const double sq = sqrt(akk);
-      const double inv = 1.0 / sq;
+      const double inv = rsqrt(akk);  // one dependent FP64 op per step instead of a root and a division
+      const double sq = akk * inv;
       rd[k] = inv;
       if (l == k) a[k] = sq;
       else if (l > k) a[k] *= inv;
@@ -150,15 +150,18 @@ __device__ void diag_block(double* A, double* W, double* vs, int k0, int kb, int
 // A holds L on return, and W's diagonal blocks hold their inverses.  Returns
 // false -- on every thread -- if a pivot is not positive or is NaN.
 // lp: n * kLpStride doubles; vs: kNb * kNb; bad: a shared int.
+// Lookahead: while warps 1.. update the trailing triangle below the next
+// diagonal block, warp 0 updates that block alone and factors it at once, so
+// each panel's serial diagonal work overlaps the previous panel's update.
 __device__ bool cholesky_blocked(double* A, double* W, int n, double* lp, double* vs, int* bad) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) *bad = 0;
   __syncthreads();
+  if (warp == 0) diag_block(A, W, vs, 0, min(kNb, n), bad);
+  __syncthreads();
   for (int k0 = 0; k0 < n; k0 += kNb) {
-    const int kb = min(kNb, n - k0);
-    if (warp == 0) diag_block(A, W, vs, k0, kb, bad);
-    __syncthreads();
     if (*bad) return false;
+    const int kb = min(kNb, n - k0);
     const int r0 = k0 + kb;
     const int rows = n - r0;
     if (rows == 0) break;
@@ -167,25 +170,51 @@ __device__ bool cholesky_blocked(double* A, double* W, int n, double* lp, double
       const int i = e / kNb, j = e % kNb;
       const double* ai = A + row_off(r0 + i) + k0;
       const double* vj = vs + j * kNb;
-      double t = 0.0;
-      for (int m = 0; m <= j; ++m) t += ai[m] * vj[m];
-      lp[i * kLpStride + j] = t;
+      double t0 = 0.0, t1 = 0.0;  // two partial sums: half the dependent chain
+      int m = 0;
+      for (; m + 1 <= j; m += 2) {
+        t0 += ai[m] * vj[m];
+        t1 += ai[m + 1] * vj[m + 1];
+      }
+      if (m <= j) t0 += ai[m] * vj[m];
+      lp[i * kLpStride + j] = t0 + t1;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < rows * kNb; e += blockDim.x) {
-      const int i = e / kNb, j = e % kNb;
-      A[row_off(r0 + i) + k0 + j] = lp[i * kLpStride + j];
-    }
-    // trailing triangle: A[r0 + i][r0 + j] -= lp[i] . lp[j], j <= i
-    for (int i = warp; i < rows; i += kWarps) {
-      const double* li = lp + i * kLpStride;
-      double* ai = A + row_off(r0 + i) + r0;
-      for (int j = lane; j <= i; j += 32) {
+    const int nb2 = min(kNb, rows);  // rows of the next diagonal block
+    if (warp == 0) {
+      // the next diagonal block: its panel rows, its own update, then its factorisation
+      for (int e = lane; e < nb2 * kNb; e += 32) {
+        const int i = e / kNb, j = e % kNb;
+        A[row_off(r0 + i) + k0 + j] = lp[i * kLpStride + j];
+      }
+      for (int e = lane; e < nb2 * nb2; e += 32) {
+        const int i = e / nb2, j = e % nb2;
+        if (j > i) continue;
+        const double* li = lp + i * kLpStride;
         const double* lj = lp + j * kLpStride;
-        double t = 0.0;
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-        for (int m = 0; m < kNb; ++m) t += li[m] * lj[m];
-        ai[j] -= t;
+        for (int m = 0; m < kNb; ++m) t[m & 3] += li[m] * lj[m];
+        A[row_off(r0 + i) + r0 + j] -= (t[0] + t[1]) + (t[2] + t[3]);
+      }
+      __syncwarp();
+      diag_block(A, W, vs, r0, nb2, bad);
+    } else {
+      // the rest: panel rows past the next block, and their trailing rows
+      for (int e = threadIdx.x - 32 + nb2 * kNb; e < rows * kNb; e += blockDim.x - 32) {
+        const int i = e / kNb, j = e % kNb;
+        A[row_off(r0 + i) + k0 + j] = lp[i * kLpStride + j];
+      }
+      for (int i = nb2 + warp - 1; i < rows; i += kWarps - 1) {
+        const double* li = lp + i * kLpStride;
+        double* ai = A + row_off(r0 + i) + r0;
+        for (int j = lane; j <= i; j += 32) {
+          const double* lj = lp + j * kLpStride;
+          double t[4] = {0.0, 0.0, 0.0, 0.0};  // four partial sums: a quarter of the dependent chain
+#pragma unroll
+          for (int m = 0; m < kNb; ++m) t[m & 3] += li[m] * lj[m];
+          ai[j] -= (t[0] + t[1]) + (t[2] + t[3]);
+        }
       }
     }
     __syncthreads();
@@ -206,27 +235,41 @@ __device__ void inverse_blocked(const double* L, double* W, int n, double* tb) {
     // phase 1: tb[r][c] = sum_{m=c}^{i0-1} L[i0 + r][m] W[m][c],  r < ib, c < i0
     for (int e = threadIdx.x; e < groups * i0; e += blockDim.x) {
       const int g = e / i0, c = e % i0;
-      double t[kRows] = {0.0, 0.0, 0.0, 0.0};
+      double t[kRows][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};  // two partial sums per row
       const double* lr[kRows];
 #pragma unroll
       for (int q = 0; q < kRows; ++q) lr[q] = L + row_off(i0 + min(g * kRows + q, ib - 1));
-      for (int m = c; m < i0; ++m) {
-        const double w = W[row_off(m) + c];
+      int m = c;
+      for (; m + 1 < i0; m += 2) {
+        const double w0 = W[row_off(m) + c], w1 = W[row_off(m + 1) + c];
 #pragma unroll
-        for (int q = 0; q < kRows; ++q) t[q] += lr[q][m] * w;
+        for (int q = 0; q < kRows; ++q) {
+          t[q][0] += lr[q][m] * w0;
+          t[q][1] += lr[q][m + 1] * w1;
+        }
+      }
+      if (m < i0) {
+        const double w0 = W[row_off(m) + c];
+#pragma unroll
+        for (int q = 0; q < kRows; ++q) t[q][0] += lr[q][m] * w0;
       }
 #pragma unroll
       for (int q = 0; q < kRows; ++q)
-        if (g * kRows + q < ib) tb[(g * kRows + q) * i0 + c] = t[q];
+        if (g * kRows + q < ib) tb[(g * kRows + q) * i0 + c] = t[q][0] + t[q][1];
     }
     __syncthreads();
     // phase 2: W[i0 + r][c] = -sum_{m <= r} V[r][m] tb[m][c]
     for (int e = threadIdx.x; e < ib * i0; e += blockDim.x) {
       const int r = e / i0, c = e % i0;
       const double* vr = W + row_off(i0 + r) + i0;
-      double t = 0.0;
-      for (int m = 0; m <= r; ++m) t += vr[m] * tb[m * i0 + c];
-      W[row_off(i0 + r) + c] = -t;
+      double t0 = 0.0, t1 = 0.0;
+      int m = 0;
+      for (; m + 1 <= r; m += 2) {
+        t0 += vr[m] * tb[m * i0 + c];
+        t1 += vr[m + 1] * tb[(m + 1) * i0 + c];
+      }
+      if (m <= r) t0 += vr[m] * tb[m * i0 + c];
+      W[row_off(i0 + r) + c] = -(t0 + t1);
     }
     __syncthreads();
   }
@@ -238,9 +281,16 @@ __device__ void lower_matvec(const double* M, const double* v, double* out, int 
     const int t = e / n, i = e % n;
     const double* mi = M + row_off(i);
     const double* vt = v + static_cast<size_t>(t) * n;
-    double s = 0.0;
-    for (int j = 0; j <= i; ++j) s += mi[j] * vt[j];
-    out[e] = s;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};  // four partial sums: a quarter of the dependent chain
+    int j = 0;
+    for (; j + 3 <= i; j += 4) {
+      s[0] += mi[j] * vt[j];
+      s[1] += mi[j + 1] * vt[j + 1];
+      s[2] += mi[j + 2] * vt[j + 2];
+      s[3] += mi[j + 3] * vt[j + 3];
+    }
+    for (; j <= i; ++j) s[0] += mi[j] * vt[j];
+    out[e] = (s[0] + s[1]) + (s[2] + s[3]);
   }
   __syncthreads();
 }
@@ -250,9 +300,16 @@ __device__ void upper_matvec(const double* M, const double* v, double* out, int 
   for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
     const int t = e / n, i = e % n;
     const double* vt = v + static_cast<size_t>(t) * n;
-    double s = 0.0;
-    for (int k = i; k < n; ++k) s += M[row_off(k) + i] * vt[k];
-    out[e] = s;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    int k = i;
+    for (; k + 3 < n; k += 4) {
+      s[0] += M[row_off(k) + i] * vt[k];
+      s[1] += M[row_off(k + 1) + i] * vt[k + 1];
+      s[2] += M[row_off(k + 2) + i] * vt[k + 2];
+      s[3] += M[row_off(k + 3) + i] * vt[k + 3];
+    }
+    for (; k < n; ++k) s[0] += M[row_off(k) + i] * vt[k];
+    out[e] = (s[0] + s[1]) + (s[2] + s[3]);
   }
   __syncthreads();
 }
