@@ -37,10 +37,20 @@ def _bip(hsi, H, W, B, T, seed):
     return cube, bip, lib[:T].copy()
 
 
-@pytest.mark.parametrize("H,W,B,T", [(64, 96, 113, 8), (37, 53, 113, 1), (48, 40, 224, 16), (33, 31, 16, 5),
-                                     (40, 64, 3, 2), (50, 50, 128, 40), (1, 7, 64, 3)])
-def test_bip_equals_bsq_bit_for_bit(hsi, orc, H, W, B, T):
+@pytest.mark.parametrize("H,W,B,T,off", [(64, 96, 113, 8, 0), (37, 53, 113, 1, 0), (48, 40, 224, 16, 0),
+                                         (33, 31, 16, 5, 0), (40, 64, 3, 2, 0), (50, 50, 128, 40, 0),
+                                         (1, 7, 64, 3, 0), (29, 41, 30, 9, 0), (45, 47, 60, 12, 0),
+                                         (20, 33, 250, 64, 0), (31, 29, 113, 8, 1), (31, 29, 64, 8, 1),
+                                         (17, 19, 30, 3, 3)])
+def test_bip_equals_bsq_bit_for_bit(hsi, orc, H, W, B, T, off):
+    """Band counts of every row layout (odd, 2 mod 4, 4 mod 8, 0 mod 8), one
+    to four target groups, and cubes whose base is not on 16 bytes (off
+    floats into an allocation: the plain-load copies)."""
     bsq, bip, lib = _bip(hsi, H, W, B, T, seed=H * 1000 + W + B)
+    if off:
+        store = torch.zeros(bip.numel() + off, device="cuda")
+        store[off:] = bip.reshape(-1)
+        bip = store[off:]
     P = H * W
     tg = torch.from_numpy(lib).cuda()
     nr = torch.from_numpy(hsi.target_norms(lib)).cuda()
