@@ -13,15 +13,18 @@
 // All arithmetic is FP64, because the factorisation of a nearly rank-6
 // covariance needs it.  One cluster of two CTAs per frame: the covariance and
 // the correlation chains run at once on two SMs; frames of a batch factor in
-// parallel.  Matrices live in shared memory as packed lower triangles when
-// they fit (B <= 128) and in the caller's workspace otherwise.  The
-// factorisation and the triangular inverse are blocked (16-column panels, the
-// diagonal blocks factored and inverted by one warp in registers), and the
-// solves use the explicit inverses, so no chain of ~B dependent steps with a
-// block barrier each remains.
+// parallel.  Up to 124 bands, the factorisation and the inverse of the factor
+// run together with the matrix in registers, one 4x4 tile per thread, in
+// panels of four columns (B / 4 steps of two block barriers each), and W
+// lands in shared memory as a packed lower triangle.  Above that the
+// factorisation and the inverse are blocked (16-column panels, the diagonal
+// blocks factored and inverted by one warp in registers), on packed triangles
+// in shared memory up to 128 bands and in the caller's workspace beyond.  The
+// solves use the explicit inverses.
 #include <cooperative_groups.h>
 
 #include "common.cuh"
+#include "launch_state.h"
 
 namespace hsi_b200 {
 namespace {
@@ -29,6 +32,10 @@ namespace {
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSmemMaxBands = 128;
+// The register-tile path: one thread per 4x4 tile of the lower triangle, up
+// to 124 rows (31 * 32 / 2 = 496 tiles).  128 rows would take 528 tiles, and
+// a 17th warp would cut the registers a thread may hold below its tile's.
+constexpr int kTileMaxBands = 124;
 constexpr int kChunk = 16;  // targets per pass through the per-target buffers
 constexpr int kNb = 16;     // panel width of the blocked factorisation
 constexpr int kLpStride = kNb + 1;  // doubles per panel row in shared memory (spreads the banks)
@@ -94,8 +101,9 @@ __device__ void fill_matrix(double* A, const double* outer, const double* mean, 
 // Step 1 (one warp): factor the diagonal block at k0 (kb <= kNb rows) in
 // registers, lane l holding row l.  Writes L_kk into A, V = L_kk^-1 into W's
 // diagonal block and densely into vs[row * kNb + col].  Sets *bad if a pivot
-// is not positive (or NaN).
-__device__ void diag_block(double* A, double* W, double* vs, int k0, int kb, int* bad) {
+// is not positive (or NaN).  Not inlined: its 48 doubles of registers would
+// otherwise be allocated across the whole kernel, whose other paths then spill.
+__device__ __noinline__ void diag_block(double* A, double* W, double* vs, int k0, int kb, int* bad) {
   const int l = threadIdx.x & 31;
   constexpr unsigned kAll = 0xffffffffu;
   double a[kNb];
@@ -275,6 +283,218 @@ __device__ void inverse_blocked(const double* L, double* W, int n, double* tb) {
   }
 }
 
+// ---- register-tile factorisation and inverse (n <= kTileMaxBands) -----------
+//
+// The right-looking blocked Cholesky and the inverse of its factor together,
+// in panels of four columns, with the matrix in registers: thread t owns the
+// 4x4 tile (I, K), I >= K, of the lower triangle.  A tile holds A (being
+// factored) until its column panel is reached, and R (becoming W = L^-1)
+// after it (the recurrences of src/linalg.cpp:105-122 and :150-162, blocked).
+// Step J, with D = chol(A_JJ) and Dinv = D^-1 (from the owner of tile (J, J)):
+//   phase 1  (J, J):        W_JJ = Dinv
+//            (J, K < J):    W_JK = Dinv R_JK           published as W^T rows
+//            (I > J, J):    L_IJ = A_IJ Dinv^T          published
+//                           R_IJ = -L_IJ Dinv
+//   phase 2  (I > J, K > J):  A_IK -= L_IJ L_KJ^T        (rank 4)
+//            (I > J, K < J):  R_IK -= L_IJ W_JK
+//            then the owner of (J+1, J+1) factors its block for the next step.
+// L rows (index >= 4J + 4) and W^T rows (index < 4J) share one published
+// panel: phase 2 is the same 64 FMAs for every tile it updates.  Two block
+// barriers per step, B / 4 steps.  Rows past n get an identity diagonal, so
+// the last panel factors as a full 4x4 block.  The matrix is formed straight
+// from the moments (M2/N, centred for the covariance, plus the loading on the
+// diagonal).  L itself is not kept: only W is used afterwards.
+
+constexpr int kPanBlock = 18;  // doubles per 4-row block of the panel: 144 bytes, 9 x 16 (conflict-free blocks)
+constexpr int kPanDoubles = 32 * kPanBlock;
+// the tile path's shared memory: the panel, Dinv, the failure flag
+constexpr int kTileShared = kPanDoubles + 16 + 2;
+
+// The Cholesky factor of the 4x4 block a (lower part) with rsqrt pivots, and
+// its inverse d (lower, upper zero).  False if a pivot is not positive or NaN.
+__device__ __forceinline__ bool factor4(const double (&a)[4][4], double (&d)[4][4]) {
+  double l[4][4], s[4];
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    double piv = a[c][c];
+#pragma unroll
+    for (int m = 0; m < c; ++m) piv = fma(-l[c][m], l[c][m], piv);
+    ok = ok && piv > 0.0;
+    s[c] = rsqrt(piv);
+    l[c][c] = piv * s[c];
+#pragma unroll
+    for (int r = c + 1; r < 4; ++r) {
+      double v = a[r][c];
+#pragma unroll
+      for (int m = 0; m < c; ++m) v = fma(-l[r][m], l[c][m], v);
+      l[r][c] = v * s[c];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+#pragma unroll
+    for (int r = 0; r < c; ++r) d[r][c] = 0.0;
+    d[c][c] = s[c];
+#pragma unroll
+    for (int r = c + 1; r < 4; ++r) {
+      double v = 0.0;
+#pragma unroll
+      for (int m = c; m < r; ++m) v = fma(l[r][m], d[m][c], v);
+      d[r][c] = -s[r] * v;
+    }
+  }
+  return ok;
+}
+
+__device__ __forceinline__ double* pan_row(double* pan, int i) { return pan + (i >> 2) * kPanBlock + (i & 3) * 4; }
+
+// sh: kTileShared doubles, 16-byte aligned.  Returns false -- on every thread,
+// at the same step -- if a pivot is not positive or is NaN.
+__device__ bool chol_inv_tiles(const double* outer, const double* mean, double N, double loading, bool centred,
+                               double* W, int n, double* sh) {
+  double* pan = sh;
+  double* dv = sh + kPanDoubles;
+  int* bad = reinterpret_cast<int*>(dv + 16);
+  const int t = threadIdx.x;
+  const int nt = (n + 3) >> 2;
+  const bool own = t < nt * (nt + 1) / 2;
+  // tiles by columns: a warp's tiles share a column panel
+  int K = 0, first = 0;
+  while (K + 1 < nt && first + (nt - K) <= t) first += nt - K++;
+  const int I = K + (t - first);
+  const int i0 = 4 * I, k0 = 4 * K;
+  double x[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = i0 + p, k = k0 + q;
+      double v = 0.0;
+      if (own && i < n && k <= i) {
+        v = outer[static_cast<size_t>(i) * n + k] / N;
+        if (centred) v -= mean[i] * mean[k];
+        if (i == k) v += loading;
+      } else if (own && i >= n && i == k) {
+        v = 1.0;  // padding: an identity block
+      }
+      x[p][q] = v;
+    }
+  if (t == 0) {  // owner of tile (0, 0)
+    double d[4][4];
+    *bad = factor4(x, d) ? 0 : 1;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) dv[r * 4 + c] = d[r][c];
+  }
+  __syncthreads();
+  for (int J = 0; J < nt; ++J) {
+    if (*bad) return false;
+    // ---- phase 1: the panel's row and column
+    if (own && (I == J || K == J)) {
+      double d[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const double2 d01 = *reinterpret_cast<const double2*>(dv + r * 4);
+        const double2 d23 = *reinterpret_cast<const double2*>(dv + r * 4 + 2);
+        d[r][0] = d01.x, d[r][1] = d01.y, d[r][2] = d23.x, d[r][3] = d23.y;
+      }
+      if (I == J && K == J) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) x[r][c] = d[r][c];
+      } else if (I == J) {
+        // W_JK = Dinv R_JK, published as rows k of W^T
+        double w[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            double v = 0.0;
+#pragma unroll
+            for (int m = 0; m <= r; ++m) v = fma(d[r][m], x[m][q], v);
+            w[r][q] = v;
+          }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          double* row = pan_row(pan, k0 + q);
+          *reinterpret_cast<double2*>(row) = make_double2(w[0][q], w[1][q]);
+          *reinterpret_cast<double2*>(row + 2) = make_double2(w[2][q], w[3][q]);
+#pragma unroll
+          for (int r = 0; r < 4; ++r) x[r][q] = w[r][q];
+        }
+      } else {
+        // L_IJ = A_IJ Dinv^T, published; then R_IJ = -L_IJ Dinv
+        double l[4][4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            double v = 0.0;
+#pragma unroll
+            for (int m = 0; m <= c; ++m) v = fma(x[p][m], d[c][m], v);
+            l[p][c] = v;
+          }
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          double* row = pan_row(pan, i0 + p);
+          *reinterpret_cast<double2*>(row) = make_double2(l[p][0], l[p][1]);
+          *reinterpret_cast<double2*>(row + 2) = make_double2(l[p][2], l[p][3]);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            double v = 0.0;
+#pragma unroll
+            for (int m = c; m < 4; ++m) v = fma(l[p][m], d[m][c], v);
+            x[p][c] = -v;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // ---- phase 2: rank-4 update of every tile below the panel's row, off its column
+    if (own && I > J && K != J) {
+      double u[4][4], v[4][4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const double* ru = pan_row(pan, i0 + p);
+        const double* rv = pan_row(pan, k0 + p);
+        const double2 u01 = *reinterpret_cast<const double2*>(ru), u23 = *reinterpret_cast<const double2*>(ru + 2);
+        const double2 v01 = *reinterpret_cast<const double2*>(rv), v23 = *reinterpret_cast<const double2*>(rv + 2);
+        u[p][0] = u01.x, u[p][1] = u01.y, u[p][2] = u23.x, u[p][3] = u23.y;
+        v[p][0] = v01.x, v[p][1] = v01.y, v[p][2] = v23.x, v[p][3] = v23.y;
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) x[p][q] = fma(-u[p][c], v[q][c], x[p][q]);
+      if (I == J + 1 && K == J + 1) {  // the next diagonal block, now final: factor it
+        double d[4][4];
+        if (!factor4(x, d)) *bad = 1;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) dv[r * 4 + c] = d[r][c];
+      }
+    }
+    __syncthreads();
+  }
+  if (own) {
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int i = i0 + p, k = k0 + q;
+        if (i < n && k <= i) W[row_off(i) + k] = x[p][q];
+      }
+  }
+  __syncthreads();
+  return true;
+}
+
 // out[t][i] = sum_{j <= i} M[i][j] v[t][j] (M packed lower), t < nt.
 __device__ void lower_matvec(const double* M, const double* v, double* out, int n, int nt) {
   for (int e = threadIdx.x; e < nt * n; e += blockDim.x) {
@@ -323,7 +543,7 @@ __device__ void upper_matvec(const double* M, const double* v, double* out, int 
 // definite first (the reference stops there), else the correlation's code.
 __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(kThreads) factor_kernel(const FactorArgs args) {
   namespace cg = cooperative_groups;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   __shared__ int s_partner_code;
   __shared__ int s_bad;
   const int f = blockIdx.x;
@@ -344,8 +564,12 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(kThreads) factor_ker
   double* buf = vec + static_cast<size_t>(kChunk) * B;
   double* lp = buf + static_cast<size_t>(kChunk) * B;
   double* vs = lp + lp_elems(B);
-  double* A = in_smem ? vs + kNb * kNb : args.scratch + (static_cast<size_t>(f) * 2 + chain) * 2 * tri(B);
-  double* W = A + tri(B);
+  double* cbuf = vs + kNb * kNb;  // the tile path's panel, Dinv and flag (kTileShared doubles, 16-byte aligned)
+  // the tile path keeps the factor in registers: only W lives in shared memory
+  const bool tiles = B <= kTileMaxBands;
+  double* A = in_smem ? cbuf + kTileShared
+                      : args.scratch + (static_cast<size_t>(f) * 2 + chain) * 2 * tri(B);
+  double* W = tiles ? A : A + tri(B);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t off_tw = static_cast<size_t>(B) + static_cast<size_t>(B) * B;
   const size_t off_tn = off_tw + static_cast<size_t>(T) * B;
@@ -360,11 +584,17 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(kThreads) factor_ker
     for (int i = threadIdx.x; i < B; i += blockDim.x) mean[i] = sum[i] / N;
     __syncthreads();
     // covariance (chain 0) or correlation (chain 1), loaded (src/linalg.cpp:56-79)
-    fill_matrix(A, outer, mean, N, args.loading, B, chain == 0);
-    if (!cholesky_blocked(A, W, B, lp, vs, &s_bad)) {
+    bool factored;
+    if (tiles) {
+      factored = chol_inv_tiles(outer, mean, N, args.loading, chain == 0, W, B, cbuf);
+    } else {
+      fill_matrix(A, outer, mean, N, args.loading, B, chain == 0);
+      factored = cholesky_blocked(A, W, B, lp, vs, &s_bad);
+      if (factored) inverse_blocked(A, W, B, lp);
+    }
+    if (!factored) {
       code = chain == 0 ? HSI_E_NOT_POSITIVE_DEFINITE : HSI_E_CORRELATION_NOT_PD;
     } else {
-      inverse_blocked(A, W, B, lp);
       if (chain == 0) {
         // outputs: mean, whitener (row-major, upper zero)
         for (int i = threadIdx.x; i < B; i += blockDim.x) {
@@ -435,7 +665,9 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(kThreads) factor_ker
 }
 
 size_t smem_bytes(int B, int /*T*/) {
-  const size_t vectors = static_cast<size_t>(B) + 2 * static_cast<size_t>(kChunk) * B + lp_elems(B) + kNb * kNb;
+  const size_t vectors =
+      static_cast<size_t>(B) + 2 * static_cast<size_t>(kChunk) * B + lp_elems(B) + kNb * kNb + kTileShared;
+  if (B <= kTileMaxBands) return sizeof(double) * (vectors + tri(B));
   if (B <= kSmemMaxBands) return sizeof(double) * (vectors + 2 * tri(B));
   return sizeof(double) * vectors;
 }
@@ -484,8 +716,7 @@ extern "C" HSI_API int hsi_build_statistics(int num_frames, int bands, int num_t
   a.scratch = static_cast<double*>(d_workspace);
   const size_t smem = smem_bytes(bands, num_targets);
   if (smem > 227 * 1024) return HSI_E_CAPACITY;
-  cudaError_t e = cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  const cudaError_t e = raise_smem_limit(factor_kernel, static_cast<int>(smem));
   if (e != cudaSuccess) return static_cast<int>(e);
   factor_kernel<<<dim3(num_frames, 2), kThreads, smem, reinterpret_cast<cudaStream_t>(stream)>>>(a);
   return static_cast<int>(cudaGetLastError());

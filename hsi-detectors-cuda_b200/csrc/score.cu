@@ -4,8 +4,8 @@
 //  * Persistent CTAs walk a static schedule of 512-pixel tiles over every
 //    frame of the launch (one frame, or a batch described by a device table).
 //  * One producer warp streams each tile's band planes into a ring of shared
-//    memory stages with 1-D bulk copies on the TMA engine (8 bands x 512 px
-//    per stage), completing on mbarriers.  Nothing but the copy engine touches
+//    memory stages with 1-D bulk copies on the TMA engine (16 FP32 or 8 FP16
+//    bands x 512 px per stage), completing on mbarriers.  Nothing but the copy engine touches
 //    the cube in HBM, and every HBM byte is read exactly once.
 //  * Up to two consumer warpgroups read each stage from shared memory: one
 //    scores the SAM library, one the CEM filters, 4 pixels per thread, with
@@ -35,24 +35,29 @@ constexpr int kTile = kGroupThreads * kPPT;
 // (twice the warps of one warpgroup at four pixels, for the same tile).
 constexpr int kFusedThreads = 256;
 constexpr int kFusedPPT = kTile / kFusedThreads;
-constexpr int kStageBands = 8;
 constexpr int kMaxTableFrames = 256;
 constexpr int kFiltersPerPass = HSI_MAX_FILTERS_PER_PASS;
 constexpr int kMaxInline = 64;  // frames whose descriptors travel inside one launch
 
 template <typename T>
 struct CubeTraits;
-// Stage ring depth: with two consumer warpgroups two CTAs fit per SM, and
-// 12 stages per SM keep ~190 KB of each SM's reads in flight.  With both
-// banks in one warpgroup three CTAs fit (the warps hide the packed FMAs'
-// latency better), with 4 stages each for FP32.
+// Stage ring: with two consumer warpgroups two CTAs fit per SM, and ~190 KB
+// of each SM's reads stay in flight.  With both banks in one warpgroup three
+// CTAs fit (the warps hide the packed FMAs' latency better), with 64 KB of
+// stages each for FP32.  FP32 stages hold 16 band planes of a tile: measured
+// on 16 resident 1024^2 x 113 frames, 16 bands x 2 stages scored a frame in
+// 114.6 us, 8 x 4 in 119.8, 8 x 5 (two CTAs) in 126.6, 12 x 3 in 121.7 and
+// 16 x 3 in 120.4 -- fewer, larger stages halve the barrier round trips per
+// band.
 template <>
 struct CubeTraits<float> {
-  static constexpr int kStages = 6;
-  static constexpr int kStagesFused = 4;
+  static constexpr int kStageBands = 16;  // band planes of a tile per stage
+  static constexpr int kStages = 3;
+  static constexpr int kStagesFused = 2;
 };
 template <>
 struct CubeTraits<__half> {
+  static constexpr int kStageBands = 8;
   static constexpr int kStages = 10;
   static constexpr int kStagesFused = 7;
 };
@@ -129,7 +134,7 @@ struct SmemLayout {
 template <typename T>
 __host__ __device__ inline SmemLayout smem_layout(int groups, int max_bands, int slots, int stages) {
   SmemLayout l;
-  l.stage_bytes = static_cast<size_t>(kStageBands) * kTile * sizeof(T);
+  l.stage_bytes = static_cast<size_t>(CubeTraits<T>::kStageBands) * kTile * sizeof(T);
   size_t off = l.stage_bytes * stages;
   l.filt_off = off;
   off += static_cast<size_t>(groups) * max_bands * slots * sizeof(float);
@@ -177,9 +182,9 @@ __device__ __forceinline__ void consume_stage(const T* stage, const float* filt2
       acc[0][1] = ffma2(v23, fa, acc[0][1]);
     }
   };
-  if (nb == kStageBands) {
+  if (nb == CubeTraits<T>::kStageBands) {
 #pragma unroll
-    for (int i = 0; i < kStageBands; ++i) band(i);
+    for (int i = 0; i < CubeTraits<T>::kStageBands; ++i) band(i);
   } else {
     for (int i = 0; i < nb; ++i) band(i);
   }
@@ -367,8 +372,8 @@ __device__ __forceinline__ void consumer_loop(const ScoreParams& prm, const int*
 #pragma unroll
     for (int k = 0; k < KG; ++k) acc[k][0] = acc[k][1] = make_float2(0.0f, 0.0f);
 
-    for (int b0 = 0; b0 < B; b0 += kStageBands) {
-      const int nb = B - b0 < kStageBands ? B - b0 : kStageBands;
+    for (int b0 = 0; b0 < B; b0 += CubeTraits<T>::kStageBands) {
+      const int nb = B - b0 < CubeTraits<T>::kStageBands ? B - b0 : CubeTraits<T>::kStageBands;
       const int slot = static_cast<int>(it % kStages);
       const uint32_t round = it / kStages;
       if (!aborted && !mbar_wait(&full[slot], round & 1u)) {
@@ -436,9 +441,9 @@ __device__ __forceinline__ void consume_stage_fused(const T* stage, const float*
       acc[k / 2 + 1][1] = ffma2(d1, fb, acc[k / 2 + 1][1]);
     }
   };
-  if (nb == kStageBands) {
+  if (nb == CubeTraits<T>::kStageBands) {
 #pragma unroll
-    for (int i = 0; i < kStageBands; ++i) band(i);
+    for (int i = 0; i < CubeTraits<T>::kStageBands; ++i) band(i);
   } else {
     for (int i = 0; i < nb; ++i) band(i);
   }
@@ -494,8 +499,8 @@ __device__ __forceinline__ void consumer_loop_fused(const ScoreParams& prm, cons
 #pragma unroll
       for (int j = 0; j < PPT; ++j) acc[k][j] = make_float2(0.0f, 0.0f);
 
-    for (int b0 = 0; b0 < B; b0 += kStageBands) {
-      const int nb = B - b0 < kStageBands ? B - b0 : kStageBands;
+    for (int b0 = 0; b0 < B; b0 += CubeTraits<T>::kStageBands) {
+      const int nb = B - b0 < CubeTraits<T>::kStageBands ? B - b0 : CubeTraits<T>::kStageBands;
       const int slot = static_cast<int>(it % kStages);
       const uint32_t round = it / kStages;
       if (!aborted && !mbar_wait(&full[slot], round & 1u)) {
@@ -630,8 +635,8 @@ __global__ void __launch_bounds__(consumer_threads<KS, KC>() + 32, fused_banks<K
         const int npx = static_cast<int>(P - p0 < kTile ? P - p0 : kTile);
         const uint32_t bytes = static_cast<uint32_t>(((npx + 7) & ~7) * sizeof(T));
         const T* cube = static_cast<const T*>(F.cube);
-        for (int b0 = 0; b0 < F.bands; b0 += kStageBands) {
-          const int nb = F.bands - b0 < kStageBands ? F.bands - b0 : kStageBands;
+        for (int b0 = 0; b0 < F.bands; b0 += CubeTraits<T>::kStageBands) {
+          const int nb = F.bands - b0 < CubeTraits<T>::kStageBands ? F.bands - b0 : CubeTraits<T>::kStageBands;
           const int slot = static_cast<int>(it % kStages);
           const uint32_t round = it / kStages;
           if (*abort_flag || !mbar_wait(&empty[slot], (round & 1u) ^ 1u)) {
