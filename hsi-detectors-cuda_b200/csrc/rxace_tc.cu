@@ -96,8 +96,8 @@ __host__ __device__ inline Smem smem_layout() {
   off += 2 * kConvWarps * kBoxPx * sizeof(float);
   s.t_off = off;                    // [kOpStages][128] ints: pixel scale exponents
   off += kOpStages * kTilePx * sizeof(int);
-  s.ops_off = off;                  // gain, offset, mean32, uu
-  off += (3 * kRows + kMaxTargetsPerPass) * sizeof(float);
+  s.ops_off = off;                  // gain, offset, mean32, uu, 1 / uu
+  off += (3 * kRows + 2 * kMaxTargetsPerPass) * sizeof(float);
   s.zz_off = off;                   // [2][128] partial |z|^2
   off += 2 * kTilePx * sizeof(float);
   s.zb_off = off;                   // [16][128] ACE numerators
@@ -224,6 +224,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   float* offset = gain + kRows;
   float* mean32 = offset + kRows;
   float* uu = mean32 + kK;
+  float* uinv = uu + kMaxTargetsPerPass;
   float* zzp = reinterpret_cast<float*>(smem + L.zz_off);
   float* zbuf = reinterpret_cast<float*>(smem + L.zb_off);
 
@@ -254,6 +255,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     fence_barrier_init();
   }
   for (int i = threadIdx.x; i < 3 * kRows + kMaxTargetsPerPass; i += blockDim.x) gain[i] = args.ops->gain[i];
+  if (threadIdx.x < kMaxTargetsPerPass) {
+    const float v = args.ops->uu[threadIdx.x];
+    uinv[threadIdx.x] = v > 0.0f ? 1.0f / v : 0.0f;
+  }
   if (warp == kWarpMma) tmem_alloc(tmem_slot, kTmemCols);
   tc_fence_before();
   __syncthreads();
@@ -545,11 +550,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (args.ace_best) best = args.ace_best[p];
             if (args.ace_target) best_t = args.ace_target[p];
           }
+          // (z.u)^2 / (|u|^2 |z|^2) as (z.u)^2 (1 / |u|^2) (1 / |z|^2): one division per
+          // pixel instead of one per target
+          const float rinv = rx > 0.0f ? 1.0f / rx : 0.0f;
           for (int k = 0; k < nt; ++k) {
             float a = 0.0f;
             if (uu[k] > 0.0f && rx > 0.0f) {
               const float zu = zbuf[k * kTilePx + px];
-              a = (zu * zu) / (uu[k] * rx);
+              a = (zu * zu) * (uinv[k] * rinv);
               if (a > best) {
                 best = a;
                 best_t = args.t0 + k;

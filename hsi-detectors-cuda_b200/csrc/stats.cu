@@ -59,6 +59,7 @@
 #include <cuda_fp16.h>
 
 #include <atomic>
+#include <type_traits>
 #include <mutex>
 
 #include "tc.cuh"
@@ -98,13 +99,12 @@ constexpr size_t kSlotElems = 2 * static_cast<size_t>(kRows) * kRows;  // INT64 
 // the float's bits are 0x4B000000 + m with m = q + 0x8080 + 2^22.  The limbs
 // are m's bytes: L2 = byte0 ^ 0x80, L1 = byte1 ^ 0x80, L0 = byte2 - 64 (the
 // 0x80 offsets make the limbs balanced), and D = 2 L0 = (2 byte2) ^ 0x80.
-// Any y outside [2^23, 2^24) (q out of range, Inf, NaN) has other exponent
-// bits: OR-ing (bits ^ 0x4B000000) over all elements and testing the top nine
-// bits detects it with one instruction per element.
+// Any y outside [2^23, 2^24) (q out of range, Inf, NaN) has other bits in
+// its top nine: byte 3 differs from 0x4B or bit 23 is set.  The converters
+// keep an OR and an AND of the packed high bytes of every four values, which
+// detects it with two instructions per four elements.
 constexpr float kMagicQ = 12615808.0f;        // 1.5 * 2^23 + 0x8080
-constexpr uint32_t kExpBits = 0x4B000000u;     // bits of 2^23
-constexpr uint32_t kZeroBits = 0x4B408080u;    // y for q = 0
-constexpr uint32_t kOnesBits = 0x4B418080u;    // y for q = 2^16 (the ones row)
+constexpr uint32_t kZeroBits = 0x4B408080u;    // y for q = 0 (the limbs of q = 2^16, the ones row: D = 2, L1 = L2 = 0)
 
 // Input stages hold one TMA box (kBoxPx pixels x 128 bands), 128 KB in all.
 template <typename T>
@@ -411,10 +411,17 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
       const FrameStats& F = t.f[f];
       const int B = F.bands;
       const int64_t P = F.pixels;
+      // Role of each slot for this frame: a band (converted), the ones row, or a
+      // row past it.  Rows past the ones row are not written at all: they only
+      // reach Gram entries (i, j) with i > B or j > B, which nothing reads, so
+      // whatever an earlier K-block or frame left there is harmless.
       float sc[kSlots], off[kSlots];
+      bool is_band[kSlots], is_ones[kSlots];
 #pragma unroll
       for (int t2 = 0; t2 < kSlots; ++t2) {
         const int b = band0 + 32 * t2;
+        is_band[t2] = b < B;
+        is_ones[t2] = b == B;
         sc[t2] = 0.0f;
         off[t2] = 0.0f;
         if (b < B) {
@@ -423,7 +430,12 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
           off[t2] = kMagicQ - F.state->shift[b] * s;  // exact when r * 2^e stays below 2^23
         }
       }
-      uint32_t chk = 0u;
+      // Range check on the packed high bytes: every converted y must have
+      // byte 3 == 0x4B (the exponent of [2^23, 2^24)) and bit 23 clear (byte
+      // 2 < 0x80).  The OR of the byte pairs catches any extra bit, the AND any
+      // missing one; bytes 0-1 of the words hold byte 2 of four values, bytes
+      // 2-3 their byte 3.
+      uint32_t chk_or = 0x4B4B0000u, chk_and = 0x4B4BFFFFu;
       // sums of L2^2 and of L2 per lane in 32 bits (at most 64 * 8 * 2^14 =
       // 2^23 between flushes), added to the frame's 64-bit counters every 64
       // K-blocks
@@ -450,10 +462,59 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
           l2s[t2] = 0;
         }
       };
+      // limbs of four converted values (y bits) of one slot, stored at byte offset o
+      auto put = [&](unsigned char* op, uint32_t o, const uint32_t (&y)[4], int t2) {
+        const uint32_t p01 = __byte_perm(y[0], y[1], 0x5140), p23 = __byte_perm(y[2], y[3], 0x5140);
+        const uint32_t h01 = __byte_perm(y[0], y[1], 0x7362), h23 = __byte_perm(y[2], y[3], 0x7362);
+        const uint32_t l2 = __byte_perm(p01, p23, 0x5410) ^ 0x80808080u;
+        const uint32_t l1 = __byte_perm(p01, p23, 0x7632) ^ 0x80808080u;
+        // byte2 <= 127 in range, so the shift carries nothing across bytes
+        const uint32_t dl = (__byte_perm(h01, h23, 0x5410) << 1) ^ 0x80808080u;
+        chk_or |= h01 | h23;
+        chk_and &= h01 & h23;
+        // signed bytes: the limbs are two's-complement INT8
+        l2sq[t2] = static_cast<unsigned int>(
+            __dp4a(static_cast<int>(l2), static_cast<int>(l2), static_cast<int>(l2sq[t2])));
+        l2s[t2] = __dp4a(static_cast<int>(l2), 0x01010101, l2s[t2]);
+        *reinterpret_cast<uint32_t*>(op + o) = dl;
+        *reinterpret_cast<uint32_t*>(op + kLimbBytes + o) = l1;
+        *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + o) = l2;
+      };
+      // One half K-block.  `full`: all 64 pixels lie in the frame (every K-block
+      // but a frame's last), so no per-pixel validity test is needed.
+      auto convert_half = [&](auto full, const T* in, int sub_off, unsigned char* op, int half, int nvalid) {
+#pragma unroll
+        for (int t2 = 0; t2 < kSlots; ++t2) {
+          const uint32_t o = (o0 + 4096u * t2) ^ (half ? 64u : 0u);
+          if (is_band[t2]) {
+            const float4 x = load4f<T>(in + (band0 + 32 * t2) * kBoxPx + sub_off + lp);
+            const float xv[4] = {x.x, x.y, x.z, x.w};
+            uint32_t y[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              y[e] = __float_as_uint(fmaf(xv[e], sc[t2], off[t2]));
+              // pixels past the frame convert as q = 0 (a fully unrolled select:
+              // no dynamic index into y[])
+              if (!decltype(full)::value && e >= nvalid) y[e] = kZeroBits;
+            }
+            put(op, o, y, t2);
+          } else if (is_ones[t2]) {
+            // the ones row: q = 2^16 (D = 2, L1 = L2 = 0) for pixels in the frame
+            uint32_t dl = 0x02020202u;
+            if (!decltype(full)::value) dl = nvalid >= 4 ? dl : (0x02020202u & ((1u << (8 * nvalid)) - 1u));
+            *reinterpret_cast<uint32_t*>(op + o) = dl;
+            *reinterpret_cast<uint32_t*>(op + kLimbBytes + o) = 0u;
+            *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + o) = 0u;
+          }
+        }
+      };
+      // K-blocks before kb_full hold 128 pixels of the frame each
+      const int64_t kb_full = F.kb_begin + P / kKB;
       int since_flush = 0;
       for (int64_t kb = walk.lo(f); kb < walk.hi(f) && !aborted; ++kb, ++i) {
         const int so = i % kOpStages;
         unsigned char* op = smem + L.op_off + static_cast<size_t>(so) * 3 * kLimbBytes;
+        const bool full = kb < kb_full;
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
           const uint32_t box = i * kBoxesPerKB + half / kHalvesPerBox;  // input box of this half
@@ -467,57 +528,12 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
             break;
           }
           const T* in = reinterpret_cast<const T*>(smem + L.in_off + static_cast<size_t>(s) * in_tile_bytes<T>());
-          const int64_t gp = (kb - F.kb_begin) * kKB + half * kHalfPx + lp;
-          const int nvalid = gp >= P ? 0 : (P - gp >= 4 ? 4 : static_cast<int>(P - gp));
-#pragma unroll
-          for (int t2 = 0; t2 < kSlots; ++t2) {
-            const int b = band0 + 32 * t2;
-            const uint32_t o = (o0 + 4096u * t2) ^ (half ? 64u : 0u);
-            if (b > B) {
-              // rows past the ones row: zero limbs (the buffer may hold another frame's rows)
-              *reinterpret_cast<uint32_t*>(op + o) = 0u;
-              *reinterpret_cast<uint32_t*>(op + kLimbBytes + o) = 0u;
-              *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + o) = 0u;
-              continue;
-            }
-            uint32_t y[4] = {kZeroBits, kZeroBits, kZeroBits, kZeroBits};
-            if (b < B) {
-              const float4 x = load4f<T>(in + b * kBoxPx + sub_off + lp);
-              const float xv[4] = {x.x, x.y, x.z, x.w};
-              if (nvalid == 4) {
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                  y[e] = __float_as_uint(fmaf(xv[e], sc[t2], off[t2]));
-                  chk |= y[e] ^ kExpBits;
-                }
-              } else {
-                // fully unrolled with a predicate: a loop bounded by nvalid would
-                // index y[] dynamically and move it to local memory
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                  if (e < nvalid) {
-                    y[e] = __float_as_uint(fmaf(xv[e], sc[t2], off[t2]));
-                    chk |= y[e] ^ kExpBits;
-                  }
-                }
-              }
-            } else if (b == B) {
-#pragma unroll
-              for (int e = 0; e < 4; ++e) y[e] = e < nvalid ? kOnesBits : kZeroBits;
-            }
-            const uint32_t p01 = __byte_perm(y[0], y[1], 0x5140), p23 = __byte_perm(y[2], y[3], 0x5140);
-            const uint32_t h01 = __byte_perm(y[0], y[1], 0x7362), h23 = __byte_perm(y[2], y[3], 0x7362);
-            const uint32_t l2 = __byte_perm(p01, p23, 0x5410) ^ 0x80808080u;
-            const uint32_t l1 = __byte_perm(p01, p23, 0x7632) ^ 0x80808080u;
-            // byte2 <= 127 in range, so the shift carries nothing across bytes
-            const uint32_t dl = (__byte_perm(h01, h23, 0x5410) << 1) ^ 0x80808080u;
-            // signed bytes: the limbs are two's-complement INT8
-            l2sq[t2] = static_cast<unsigned int>(
-                __dp4a(static_cast<int>(l2), static_cast<int>(l2), static_cast<int>(l2sq[t2])));
-            l2s[t2] = __dp4a(static_cast<int>(l2), 0x01010101, l2s[t2]);
-            *reinterpret_cast<uint32_t*>(op + o) = dl;
-            *reinterpret_cast<uint32_t*>(op + kLimbBytes + o) = l1;
-            *reinterpret_cast<uint32_t*>(op + 2 * kLimbBytes + o) = l2;
+          if (full) {
+            convert_half(std::true_type{}, in, sub_off, op, half, 4);
+          } else {
+            const int64_t gp = (kb - F.kb_begin) * kKB + half * kHalfPx + lp;
+            const int nvalid = gp >= P ? 0 : (P - gp >= 4 ? 4 : static_cast<int>(P - gp));
+            convert_half(std::false_type{}, in, sub_off, op, half, nvalid);
           }
           __syncwarp();
           if (lane == 0 && sub_off + kHalfPx == kBoxPx) mbar_arrive(&in_empty[s]);
@@ -534,7 +550,8 @@ __global__ void __launch_bounds__(kThreads, 1) stats_gemm_kernel(const __grid_co
       }
       // end of the piece: the remaining L2^2 sums and the range check
       flush_l2();
-      if (__any_sync(0xffffffffu, (chk >> 23) != 0u) && lane == 0) atomicOr(&F.state->flags, 1);
+      const bool bad = (chk_or & 0xFFFF8080u) != 0x4B4B0000u || (chk_and >> 16) != 0x4B4Bu;
+      if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&F.state->flags, 1);
     }
   } else {
     // ---------------- epilogue ----------------
