@@ -39,15 +39,23 @@ struct Frame {
 }  // namespace
 
 struct hsi_batch {
+  // Per-frame chains (factor, then RX/ACE) run on kLanes streams forked from
+  // the caller's stream, and the SAM scorer on one more, so frames overlap:
+  // a frame's FP64 factor occupies two SMs and a small frame's RX/ACE only
+  // part of the GPU.  Each lane has its own factor and RX/ACE workspace.
+  static constexpr int kLanes = 4;
   std::vector<Frame> frames;
   hsi_batch_options opt{};
   std::vector<void*> allocations;
   void* stats_ws = nullptr;
   size_t stats_bytes = 0;
-  void* factor_ws = nullptr;
+  void* factor_ws[kLanes] = {};
   size_t factor_bytes = 0;
-  void* rx_ws = nullptr;
+  void* rx_ws[kLanes] = {};
   size_t rx_bytes = 0;
+  std::vector<int> lane_of;            // lane of each frame's chain
+  cudaStream_t lanes[kLanes + 1] = {};  // [kLanes]: the scorer's
+  cudaEvent_t ev_cubes = nullptr, ev_moments = nullptr, ev_done[kLanes + 1] = {};
   void* det_ws = nullptr;
   size_t det_bytes = 0;
   uint32_t* all_counts = nullptr;
@@ -64,7 +72,24 @@ struct hsi_batch {
   ~hsi_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+    for (cudaStream_t l : lanes)
+      if (l) cudaStreamDestroy(l);
+    for (cudaEvent_t e : ev_done)
+      if (e) cudaEventDestroy(e);
+    if (ev_cubes) cudaEventDestroy(ev_cubes);
+    if (ev_moments) cudaEventDestroy(ev_moments);
     for (void* p : allocations) cudaFree(p);
+  }
+
+  int make_lanes() {
+    for (cudaStream_t& l : lanes)
+      if (cudaStreamCreateWithFlags(&l, cudaStreamNonBlocking) != cudaSuccess) return HSI_E_INVALID;
+    for (cudaEvent_t& e : ev_done)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return HSI_E_INVALID;
+    if (cudaEventCreateWithFlags(&ev_cubes, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev_moments, cudaEventDisableTiming) != cudaSuccess)
+      return HSI_E_INVALID;
+    return HSI_OK;
   }
 
   template <typename T>
@@ -77,14 +102,14 @@ struct hsi_batch {
     return HSI_OK;
   }
 
-  int rx_ace(Frame& f, bool tensor_core, cudaStream_t s) {
+  int rx_ace(Frame& f, bool tensor_core, int lane, cudaStream_t s) {
     const hsi_batch_frame& sp = f.spec;
     const hsi_stream_t hs = reinterpret_cast<hsi_stream_t>(s);
     if (tensor_core)
       return hsi_rx_ace(f.cube, sp.height, sp.width, sp.bands, sp.dtype, f.stride, f.stats64, sp.num_targets, f.rx,
-                        f.ace_best, f.ace_target, nullptr, f.P, rx_ws, rx_bytes, hs);
+                        f.ace_best, f.ace_target, nullptr, f.P, rx_ws[lane], rx_bytes, hs);
     return hsi_rx_ace_simt(f.cube, sp.height, sp.width, sp.bands, sp.dtype, f.stride, f.stats64, sp.num_targets, f.rx,
-                           f.ace_best, f.ace_target, nullptr, f.P, rx_ws, rx_bytes, hs);
+                           f.ace_best, f.ace_target, nullptr, f.P, rx_ws[lane], rx_bytes, hs);
   }
 
   int score(int cps, cudaStream_t s) {
@@ -97,6 +122,11 @@ struct hsi_batch {
     return HSI_OK;
   }
 
+  // The plan on the caller's stream s: demosaic; then the scorer on its lane
+  // (it needs only the cubes) while s runs the batched moments; then each
+  // frame's factor and RX/ACE on the frame's lane; s waits for every lane and
+  // runs the detection launches.  Every fork is joined before return (also on
+  // errors), so a capture of s records the whole plan.
   int run(cudaStream_t s) {
     const hsi_stream_t hs = reinterpret_cast<hsi_stream_t>(s);
     for (Frame& f : frames) {
@@ -106,22 +136,40 @@ struct hsi_batch {
                                   f.stride, hs);
       if (rc != HSI_OK) return rc;
     }
-    int rc = hsi_scene_moments_batch(moment_jobs.data(), static_cast<int>(moment_jobs.size()), stats_ws, stats_bytes,
-                                     hs);
-    if (rc != HSI_OK) return rc;
-    for (Frame& f : frames) {
-      const hsi_batch_frame& sp = f.spec;
-      rc = hsi_build_statistics(1, sp.bands, sp.num_targets, opt.loading, f.moments, f.targets, 0, f.stats64, nullptr,
-                                nullptr, f.status, factor_ws, factor_bytes, hs);
-      if (rc != HSI_OK) return rc;
+    cudaError_t e = cudaEventRecord(ev_cubes, s);
+    if (e != cudaSuccess) return static_cast<int>(e);
+    int rc = HSI_OK;
+    bool forked[kLanes + 1] = {};
+    if ((e = cudaStreamWaitEvent(lanes[kLanes], ev_cubes, 0)) == cudaSuccess) {
+      forked[kLanes] = true;
+      rc = score(score_ctas_per_sm, lanes[kLanes]);
     }
-    rc = score(score_ctas_per_sm, s);
-    if (rc != HSI_OK) return rc;
-    for (Frame& f : frames) {
-      rc = rx_ace(f, f.tensor_core_rx, s);
-      if (rc != HSI_OK) return rc;
+    if (rc == HSI_OK && e == cudaSuccess)
+      rc = hsi_scene_moments_batch(moment_jobs.data(), static_cast<int>(moment_jobs.size()), stats_ws, stats_bytes, hs);
+    if (rc == HSI_OK && e == cudaSuccess) e = cudaEventRecord(ev_moments, s);
+    for (int l = 0; l < kLanes && rc == HSI_OK && e == cudaSuccess; ++l) {
+      if ((e = cudaStreamWaitEvent(lanes[l], ev_moments, 0)) != cudaSuccess) break;
+      forked[l] = true;
+      const hsi_stream_t hl = reinterpret_cast<hsi_stream_t>(lanes[l]);
+      for (size_t i = 0; i < frames.size() && rc == HSI_OK; ++i) {
+        if (lane_of[i] != l) continue;
+        Frame& f = frames[i];
+        const hsi_batch_frame& sp = f.spec;
+        rc = hsi_build_statistics(1, sp.bands, sp.num_targets, opt.loading, f.moments, f.targets, 0, f.stats64,
+                                  nullptr, nullptr, f.status, factor_ws[l], factor_bytes, hl);
+        if (rc == HSI_OK) rc = rx_ace(f, f.tensor_core_rx, l, lanes[l]);
+      }
     }
-    const cudaError_t e = cudaMemsetAsync(all_counts, 0, sizeof(uint32_t) * 3 * frames.size(), s);
+    // join every lane that was forked
+    for (int l = 0; l <= kLanes; ++l) {
+      if (!forked[l]) continue;
+      cudaError_t j = cudaEventRecord(ev_done[l], lanes[l]);
+      if (j == cudaSuccess) j = cudaStreamWaitEvent(s, ev_done[l], 0);
+      if (e == cudaSuccess) e = j;
+    }
+    if (rc != HSI_OK) return rc;
+    if (e != cudaSuccess) return static_cast<int>(e);
+    e = cudaMemsetAsync(all_counts, 0, sizeof(uint32_t) * 3 * frames.size(), s);
     if (e != cudaSuccess) return static_cast<int>(e);
     for (size_t j0 = 0; j0 < jobs.size(); j0 += HSI_MAX_DETECT_JOBS) {
       const int n = static_cast<int>(std::min<size_t>(HSI_MAX_DETECT_JOBS, jobs.size() - j0));
@@ -278,12 +326,33 @@ int build(hsi_batch* bt, const hsi_batch_frame* frames, int n) {
   unsigned char* p = nullptr;
   rc = bt->alloc(&p, std::max<size_t>(bt->stats_bytes, 256));
   bt->stats_ws = p;
-  if (rc == HSI_OK) rc = bt->alloc(&p, std::max<size_t>(bt->factor_bytes, 256));
-  bt->factor_ws = p;
-  if (rc == HSI_OK) rc = bt->alloc(&p, std::max<size_t>(bt->rx_bytes, 256));
-  bt->rx_ws = p;
+  for (int l = 0; l < hsi_batch::kLanes && rc == HSI_OK; ++l) {
+    rc = bt->alloc(&p, std::max<size_t>(bt->factor_bytes, 256));
+    bt->factor_ws[l] = p;
+    if (rc == HSI_OK) rc = bt->alloc(&p, std::max<size_t>(bt->rx_bytes, 256));
+    bt->rx_ws[l] = p;
+  }
   if (rc == HSI_OK) rc = bt->alloc(&p, std::max<size_t>(bt->det_bytes, 256));
   bt->det_ws = p;
+  if (rc == HSI_OK) rc = bt->make_lanes();
+  // Frames to lanes, largest chain first onto the least loaded lane; the cost
+  // of a chain is its RX/ACE arithmetic, pixels x bands x (bands + targets).
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  auto cost = [&](int i) {
+    const hsi_batch_frame& sp = bt->frames[i].spec;
+    return static_cast<double>(bt->frames[i].P) * sp.bands * (sp.bands + sp.num_targets);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+  bt->lane_of.assign(n, 0);
+  double load[hsi_batch::kLanes] = {};
+  for (int i : order) {
+    int l = 0;
+    for (int k = 1; k < hsi_batch::kLanes; ++k)
+      if (load[k] < load[l]) l = k;
+    bt->lane_of[i] = l;
+    load[l] += cost(i);
+  }
   return rc;
 }
 
@@ -309,9 +378,9 @@ int autotune(hsi_batch* bt) {
   }
   for (Frame& f : bt->frames) {
     if (rc != HSI_OK || f.spec.bands > 127) continue;
-    rc = bt->rx_ace(f, true, s);  // warm
-    const float tc = time_ms([&] { return bt->rx_ace(f, true, s); }, 2, s, &rc);
-    const float plain = time_ms([&] { return bt->rx_ace(f, false, s); }, 2, s, &rc);
+    rc = bt->rx_ace(f, true, 0, s);  // warm
+    const float tc = time_ms([&] { return bt->rx_ace(f, true, 0, s); }, 2, s, &rc);
+    const float plain = time_ms([&] { return bt->rx_ace(f, false, 0, s); }, 2, s, &rc);
     f.tensor_core_rx = tc <= plain;
   }
   cudaEventRecord(b, s);

@@ -413,22 +413,24 @@ __device__ __forceinline__ void consumer_loop(const ScoreParams& prm, const int*
   }
 }
 
-// Fused consumer: two warpgroups score the SAM and the CEM bank together, so
-// each pixel leaves shared memory once for all KS + KC filters.  The bank is
+// Fused consumer: two warpgroups score the SAM and the CEM bank (either may be
+// empty) together, so each pixel leaves shared memory once for all KS + KC
+// filters.  The bank is
 // stored band-major without duplication, [b][KS SAM | KC CEM]; accumulators
 // are filter pairs per pixel, (acc_k, acc_k+1) += (x, x) * (f_k, f_k+1), the
 // pixel duplicated in a register pair for the packed FMA.  Two pixels per
 // thread keep the accumulators at 2 * (KS + KC) registers, so 256 consumer
 // threads fit per CTA at three CTAs per SM (twice the warps of one warpgroup
 // at four pixels per thread, to hide the shared-memory and FMA latencies).
-template <typename T, int K>
+template <typename T, int K, bool kNorm>
 __device__ __forceinline__ void consume_stage_fused(const T* stage, const float* filt, int nb, int tid,
                                                     float2 (&acc)[K / 2][kFusedPPT], float2& nrm) {
   static_assert(kFusedPPT == 2, "two pixels per fused consumer thread");
+  static_assert(K % 4 == 0, "filters in groups of four");
   const T* src = stage + tid * kFusedPPT;
   auto band = [&](int i) {
     const float2 v = load2<T>(src + i * kTile);
-    nrm = ffma2(v, v, nrm);
+    if constexpr (kNorm) nrm = ffma2(v, v, nrm);
     const float2 d0 = make_float2(v.x, v.x), d1 = make_float2(v.y, v.y);
     const float* fr = filt + i * K;
 #pragma unroll
@@ -510,7 +512,7 @@ __device__ __forceinline__ void consumer_loop_fused(const ScoreParams& prm, cons
       }
       if (active && !aborted) {
         const T* stage = reinterpret_cast<const T*>(smem + slot * stage_bytes);
-        consume_stage_fused<T, K>(stage, filt + b0 * K, nb, tid, acc, nrm);
+        consume_stage_fused<T, K, (KS > 0)>(stage, filt + b0 * K, nb, tid, acc, nrm);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[slot]);
@@ -521,33 +523,42 @@ __device__ __forceinline__ void consumer_loop_fused(const ScoreParams& prm, cons
       const int64_t rem = P - p;
       const int valid = rem <= 0 ? 0 : (rem >= PPT ? PPT : static_cast<int>(rem));
       if (valid > 0) {
-        if (n_s > 0) {
-          float a[KS][PPT];
+        if constexpr (KS > 0) {
+          if (n_s > 0) {
+            float a[KS][PPT];
 #pragma unroll
-          for (int k = 0; k < KS; ++k)
+            for (int k = 0; k < KS; ++k)
 #pragma unroll
-            for (int j = 0; j < PPT; ++j) a[k][j] = (k & 1) ? acc[k / 2][j].y : acc[k / 2][j].x;
-          const float n[PPT] = {nrm.x, nrm.y};
-          sam_epilogue<KS, PPT>(F, prm.pass, n_s, p, valid, a, n, scale);
+              for (int j = 0; j < PPT; ++j) a[k][j] = (k & 1) ? acc[k / 2][j].y : acc[k / 2][j].x;
+            const float n[PPT] = {nrm.x, nrm.y};
+            sam_epilogue<KS, PPT>(F, prm.pass, n_s, p, valid, a, n, scale);
+          }
         }
-        if (n_c > 0) {
-          float a[KC][PPT];
+        if constexpr (KC > 0) {
+          if (n_c > 0) {
+            float a[KC][PPT];
 #pragma unroll
-          for (int k = 0; k < KC; ++k)
+            for (int k = 0; k < KC; ++k)
 #pragma unroll
-            for (int j = 0; j < PPT; ++j)
-              a[k][j] = ((KS + k) & 1) ? acc[(KS + k) / 2][j].y : acc[(KS + k) / 2][j].x;
-          cem_epilogue<KC, PPT>(F, prm.pass, n_c, p, valid, a);
+              for (int j = 0; j < PPT; ++j)
+                a[k][j] = ((KS + k) & 1) ? acc[(KS + k) / 2][j].y : acc[(KS + k) / 2][j].x;
+            cem_epilogue<KC, PPT>(F, prm.pass, n_c, p, valid, a);
+          }
         }
       }
     }
   }
 }
 
-// Both banks in one warpgroup: 4 or 8 filters of each kind.
+// One bank layout for both kinds: 0, 4, 8 or 16 filters of each kind, at most
+// 16 in all (two pixels per thread keep the accumulators at 2 (KS + KC)
+// registers).  Other counts (a single filter, or more than 16 in all) take one
+// warpgroup per kind.
 template <int KS, int KC>
 constexpr bool fused_banks() {
-  return (KS == 4 || KS == 8) && (KC == 4 || KC == 8);
+  constexpr bool ks = KS == 0 || KS == 4 || KS == 8 || KS == 16;
+  constexpr bool kc = KC == 0 || KC == 4 || KC == 8 || KC == 16;
+  return ks && kc && KS + KC > 0 && KS + KC <= 16;
 }
 
 // Kernel: KS SAM filters and KC CEM filters per pass (0 = that warpgroup is
