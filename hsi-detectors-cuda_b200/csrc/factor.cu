@@ -19,8 +19,10 @@
 // lands in shared memory as a packed lower triangle.  Above that the
 // factorisation and the inverse are blocked (16-column panels, the diagonal
 // blocks factored and inverted by one warp in registers), on packed triangles
-// in shared memory up to 128 bands and in the caller's workspace beyond.  The
-// solves use the explicit inverses.
+// in shared memory up to 128 bands; up to 238 bands one packed triangle in
+// shared memory turns from the matrix into L and then into W in place (the
+// target vectors in the caller's workspace), and beyond that the matrices
+// live in the workspace.  The solves use the explicit inverses.
 #include <cooperative_groups.h>
 
 #include "common.cuh"
@@ -32,6 +34,9 @@ namespace {
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSmemMaxBands = 128;
+// Shared memory a CTA may hold on sm_100 (opt-in), less the kernel's static
+// shared variables and a margin.
+constexpr size_t kSmemLimit = 232448 - 64;
 // The register-tile path: one thread per 4x4 tile of the lower triangle, up
 // to 124 rows (31 * 32 / 2 = 496 tiles).  128 rows would take 528 tiles, and
 // a 17th warp would cut the registers a thread may hold below its tile's.
@@ -84,6 +89,17 @@ __device__ void fill_matrix(double* A, const double* outer, const double* mean, 
   }
   __syncthreads();
 }
+
+// The in-place path (kSmemMaxBands < B <= kHybridMaxBands): mean[B], the
+// diagonal block's inverse and the packed matrix in shared memory, followed by
+// the inverse's block-row buffer (kNb x the last block row's start) when it
+// still fits; the target vectors, and that buffer otherwise, in the workspace.
+__host__ __device__ inline size_t last_block_row(int n) { return static_cast<size_t>((n - 1) / kNb) * kNb; }
+__host__ __device__ inline size_t inplace_core(int n) { return static_cast<size_t>(n) + kNb * kNb + tri(n); }
+__host__ __device__ inline bool inplace_tb_in_smem(int n) {
+  return sizeof(double) * (inplace_core(n) + kNb * last_block_row(n)) <= kSmemLimit;
+}
+constexpr int kHybridMaxBands = 238;  // the largest n with inplace_core(n) doubles within kSmemLimit
 
 // ---- blocked Cholesky and triangular inverse (panels of kNb columns) --------
 //
@@ -144,6 +160,7 @@ __device__ __noinline__ void diag_block(double* A, double* W, double* vs, int k0
     for (int m = 0; m < kNb; ++m)
       if (m <= l) ar[m] = a[m];
   }
+  __syncwarp();  // L_kk before V over it, when W is A (the in-place path)
   if (l < kNb) {
 #pragma unroll
     for (int i = 0; i < kNb; ++i) {
@@ -218,6 +235,81 @@ __device__ bool cholesky_blocked(double* A, double* W, int n, double* lp, double
         double* ai = A + row_off(r0 + i) + r0;
         for (int j = lane; j <= i; j += 32) {
           const double* lj = lp + j * kLpStride;
+          double t[4] = {0.0, 0.0, 0.0, 0.0};  // four partial sums: a quarter of the dependent chain
+#pragma unroll
+          for (int m = 0; m < kNb; ++m) t[m & 3] += li[m] * lj[m];
+          ai[j] -= (t[0] + t[1]) + (t[2] + t[3]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
+// The same blocked Cholesky with the matrix alone in shared memory (the
+// packed triangle of up to kHybridMaxBands rows, with no room for a panel
+// buffer beside it): each panel L_21 = A_21 V^T is formed in place, one
+// thread per row with the row's kNb values in registers, and the trailing
+// update reads L_21 from A.  The diagonal blocks receive V_kk = L_kk^-1 over
+// L_kk (nothing reads L_kk afterwards), so inverse_blocked(A, A, ...) then
+// turns A into W in place.
+__device__ bool cholesky_inplace(double* A, int n, double* vs, int* bad) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) *bad = 0;
+  __syncthreads();
+  if (warp == 0) diag_block(A, A, vs, 0, min(kNb, n), bad);
+  __syncthreads();
+  for (int k0 = 0; k0 < n; k0 += kNb) {
+    if (*bad) return false;
+    const int kb = min(kNb, n - k0);
+    const int r0 = k0 + kb;
+    const int rows = n - r0;
+    if (rows == 0) break;
+    // panel, in place (kb == kNb here): row i's values are read into registers before any is written
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+      double* ai = A + row_off(r0 + i) + k0;
+      double a[kNb];
+#pragma unroll
+      for (int m = 0; m < kNb; ++m) a[m] = ai[m];
+#pragma unroll
+      for (int j = 0; j < kNb; ++j) {
+        const double* vj = vs + j * kNb;
+        double t0 = 0.0, t1 = 0.0;  // two partial sums: half the dependent chain
+#pragma unroll
+        for (int m = 0; m <= j; ++m) {
+          if (m & 1)
+            t1 += a[m] * vj[m];
+          else
+            t0 += a[m] * vj[m];
+        }
+        ai[j] = t0 + t1;
+      }
+    }
+    __syncthreads();
+    const int nb2 = min(kNb, rows);  // rows of the next diagonal block
+    if (warp == 0) {
+      // the next diagonal block's own update, then its factorisation
+      for (int e = lane; e < nb2 * nb2; e += 32) {
+        const int i = e / nb2, j = e % nb2;
+        if (j > i) continue;
+        const double* li = A + row_off(r0 + i) + k0;
+        const double* lj = A + row_off(r0 + j) + k0;
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int m = 0; m < kNb; ++m) t[m & 3] += li[m] * lj[m];
+        A[row_off(r0 + i) + r0 + j] -= (t[0] + t[1]) + (t[2] + t[3]);
+      }
+      __syncwarp();
+      diag_block(A, A, vs, r0, nb2, bad);
+    } else {
+      // the trailing rows past the next block (their columns r0.. only; the
+      // panel columns k0.. that warp 0 reads are not written here)
+      for (int i = nb2 + warp - 1; i < rows; i += kWarps - 1) {
+        const double* li = A + row_off(r0 + i) + k0;
+        double* ai = A + row_off(r0 + i) + r0;
+        for (int j = lane; j <= i; j += 32) {
+          const double* lj = A + row_off(r0 + j) + k0;
           double t[4] = {0.0, 0.0, 0.0, 0.0};  // four partial sums: a quarter of the dependent chain
 #pragma unroll
           for (int m = 0; m < kNb; ++m) t[m & 3] += li[m] * lj[m];
@@ -556,9 +648,11 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(kThreads) factor_ker
   float* out32 = args.stats32 ? args.stats32 + f * per : nullptr;
   float* cem32 = args.cem32 ? args.cem32 + static_cast<size_t>(f) * T * B : nullptr;
   const bool in_smem = B <= kSmemMaxBands;
+  const bool inplace = !in_smem && B <= kHybridMaxBands;
   // smem: mean[B], two chunk buffers of kChunk x B, the panel / block-row
   // buffer, the diagonal block's inverse, then the packed matrices (in the
-  // workspace when B is large)
+  // workspace when B is large).  The in-place path keeps only mean, the
+  // diagonal block's inverse and one matrix in shared memory.
   double* mean = smem;
   double* vec = mean + B;
   double* buf = vec + static_cast<size_t>(kChunk) * B;
@@ -567,9 +661,16 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(kThreads) factor_ker
   double* cbuf = vs + kNb * kNb;  // the tile path's panel, Dinv and flag (kTileShared doubles, 16-byte aligned)
   // the tile path keeps the factor in registers: only W lives in shared memory
   const bool tiles = B <= kTileMaxBands;
-  double* A = in_smem ? cbuf + kTileShared
-                      : args.scratch + (static_cast<size_t>(f) * 2 + chain) * 2 * tri(B);
+  double* ws = args.scratch + (static_cast<size_t>(f) * 2 + chain) * 2 * tri(B);
+  double* A = in_smem ? cbuf + kTileShared : ws;
   double* W = tiles ? A : A + tri(B);
+  if (inplace) {
+    vs = mean + B;
+    A = W = vs + kNb * kNb;
+    vec = ws;
+    buf = vec + static_cast<size_t>(kChunk) * B;
+    lp = inplace_tb_in_smem(B) ? A + tri(B) : buf + static_cast<size_t>(kChunk) * B;
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t off_tw = static_cast<size_t>(B) + static_cast<size_t>(B) * B;
   const size_t off_tn = off_tw + static_cast<size_t>(T) * B;
@@ -587,6 +688,10 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(kThreads) factor_ker
     bool factored;
     if (tiles) {
       factored = chol_inv_tiles(outer, mean, N, args.loading, chain == 0, W, B, cbuf);
+    } else if (inplace) {
+      fill_matrix(A, outer, mean, N, args.loading, B, chain == 0);
+      factored = cholesky_inplace(A, B, vs, &s_bad);
+      if (factored) inverse_blocked(A, A, B, lp);
     } else {
       fill_matrix(A, outer, mean, N, args.loading, B, chain == 0);
       factored = cholesky_blocked(A, W, B, lp, vs, &s_bad);
@@ -669,6 +774,8 @@ size_t smem_bytes(int B, int /*T*/) {
       static_cast<size_t>(B) + 2 * static_cast<size_t>(kChunk) * B + lp_elems(B) + kNb * kNb + kTileShared;
   if (B <= kTileMaxBands) return sizeof(double) * (vectors + tri(B));
   if (B <= kSmemMaxBands) return sizeof(double) * (vectors + 2 * tri(B));
+  if (B <= kHybridMaxBands)
+    return sizeof(double) * (inplace_core(B) + (inplace_tb_in_smem(B) ? kNb * last_block_row(B) : 0));
   return sizeof(double) * vectors;
 }
 

@@ -101,7 +101,11 @@ def _fp64_moments_on_device(orc, host):
     return torch.from_numpy(np.concatenate([s, o.reshape(-1), [n]])).cuda(), (s, o, n)
 
 
-@pytest.mark.parametrize("B,T", [(12, 2), (113, 8), (128, 16), (224, 16)])
+# 129..238 bands: one packed triangle in shared memory turned into L and then W
+# in place (224: the inverse's block-row buffer in shared memory too; 225 and
+# 238: in the workspace); 239 and 254: the matrices in the workspace.
+@pytest.mark.parametrize("B,T", [(12, 2), (113, 8), (128, 16), (129, 4), (176, 3), (224, 16), (225, 16), (238, 5),
+                                 (239, 2), (254, 16)])
 def test_factor_matches_fp64_oracle(hsi, orc, B, T):
     H, W = 48, 64
     sc = hsi.scene(B, n_targets=T, target_frac=0.01, frame_seed=B + T)
