@@ -47,6 +47,9 @@ constexpr int kLpStride = kNb + 1;  // doubles per panel row in shared memory (s
 
 __host__ __device__ inline size_t tri(int n) { return static_cast<size_t>(n) * (n + 1) / 2; }
 __device__ __forceinline__ size_t row_off(int i) { return static_cast<size_t>(i) * (i + 1) / 2; }
+// The same offset in 32 bits, for triangles in shared memory (at most 256 rows):
+// the in-place path's loops then carry 32-bit shared-memory addresses.
+__device__ __forceinline__ unsigned ro32(int i) { return static_cast<unsigned>(i) * static_cast<unsigned>(i + 1) / 2u; }
 // doubles of the panel buffer (n rows of kLpStride), which the inverse reuses
 // as its block-row buffer (kNb rows of up to n columns)
 __host__ __device__ inline size_t lp_elems(int n) {
@@ -254,7 +257,7 @@ __device__ bool cholesky_blocked(double* A, double* W, int n, double* lp, double
 // update reads L_21 from A.  The diagonal blocks receive V_kk = L_kk^-1 over
 // L_kk (nothing reads L_kk afterwards), so inverse_blocked(A, A, ...) then
 // turns A into W in place.
-__device__ bool cholesky_inplace(double* A, int n, double* vs, int* bad) {
+__device__ __forceinline__ bool cholesky_inplace(double* A, int n, double* vs, int* bad) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) *bad = 0;
   __syncthreads();
@@ -268,7 +271,7 @@ __device__ bool cholesky_inplace(double* A, int n, double* vs, int* bad) {
     if (rows == 0) break;
     // panel, in place (kb == kNb here): row i's values are read into registers before any is written
     for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-      double* ai = A + row_off(r0 + i) + k0;
+      double* ai = A + ro32(r0 + i) + k0;
       double a[kNb];
 #pragma unroll
       for (int m = 0; m < kNb; ++m) a[m] = ai[m];
@@ -293,12 +296,12 @@ __device__ bool cholesky_inplace(double* A, int n, double* vs, int* bad) {
       for (int e = lane; e < nb2 * nb2; e += 32) {
         const int i = e / nb2, j = e % nb2;
         if (j > i) continue;
-        const double* li = A + row_off(r0 + i) + k0;
-        const double* lj = A + row_off(r0 + j) + k0;
+        const double* li = A + ro32(r0 + i) + k0;
+        const double* lj = A + ro32(r0 + j) + k0;
         double t[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int m = 0; m < kNb; ++m) t[m & 3] += li[m] * lj[m];
-        A[row_off(r0 + i) + r0 + j] -= (t[0] + t[1]) + (t[2] + t[3]);
+        A[ro32(r0 + i) + r0 + j] -= (t[0] + t[1]) + (t[2] + t[3]);
       }
       __syncwarp();
       diag_block(A, A, vs, r0, nb2, bad);
@@ -306,10 +309,10 @@ __device__ bool cholesky_inplace(double* A, int n, double* vs, int* bad) {
       // the trailing rows past the next block (their columns r0.. only; the
       // panel columns k0.. that warp 0 reads are not written here)
       for (int i = nb2 + warp - 1; i < rows; i += kWarps - 1) {
-        const double* li = A + row_off(r0 + i) + k0;
-        double* ai = A + row_off(r0 + i) + r0;
+        const double* li = A + ro32(r0 + i) + k0;
+        double* ai = A + ro32(r0 + i) + r0;
         for (int j = lane; j <= i; j += 32) {
-          const double* lj = A + row_off(r0 + j) + k0;
+          const double* lj = A + ro32(r0 + j) + k0;
           double t[4] = {0.0, 0.0, 0.0, 0.0};  // four partial sums: a quarter of the dependent chain
 #pragma unroll
           for (int m = 0; m < kNb; ++m) t[m & 3] += li[m] * lj[m];
@@ -370,6 +373,58 @@ __device__ void inverse_blocked(const double* L, double* W, int n, double* tb) {
       }
       if (m <= r) t0 += vr[m] * tb[m * i0 + c];
       W[row_off(i0 + r) + c] = -(t0 + t1);
+    }
+    __syncthreads();
+  }
+}
+
+// inverse_blocked for the in-place path: W over L in one shared-memory
+// triangle (the same sums in the same order, so the same bits), with 32-bit
+// shared-memory offsets and the block-row buffer tb in shared memory or the
+// workspace.
+__device__ __forceinline__ void inverse_inplace(double* A, int n, double* tb) {
+  constexpr int kRows = 4;
+  for (int i0 = kNb; i0 < n; i0 += kNb) {
+    const int ib = min(kNb, n - i0);
+    const int groups = (ib + kRows - 1) / kRows;
+    for (int e = threadIdx.x; e < groups * i0; e += blockDim.x) {
+      const int g = e / i0, c = e % i0;
+      double t[kRows][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+      unsigned lr[kRows];
+#pragma unroll
+      for (int q = 0; q < kRows; ++q) lr[q] = ro32(i0 + min(g * kRows + q, ib - 1));
+      int m = c;
+      unsigned wm = ro32(m) + c;  // A[m][c]: row m + 1 starts m + 1 doubles after row m
+      for (; m + 1 < i0; m += 2) {
+        const double w0 = A[wm], w1 = A[wm + m + 1];
+        wm += 2 * m + 3;
+#pragma unroll
+        for (int q = 0; q < kRows; ++q) {
+          t[q][0] += A[lr[q] + m] * w0;
+          t[q][1] += A[lr[q] + m + 1] * w1;
+        }
+      }
+      if (m < i0) {
+        const double w0 = A[wm];
+#pragma unroll
+        for (int q = 0; q < kRows; ++q) t[q][0] += A[lr[q] + m] * w0;
+      }
+#pragma unroll
+      for (int q = 0; q < kRows; ++q)
+        if (g * kRows + q < ib) tb[(g * kRows + q) * i0 + c] = t[q][0] + t[q][1];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < ib * i0; e += blockDim.x) {
+      const int r = e / i0, c = e % i0;
+      const unsigned vr = ro32(i0 + r) + i0;
+      double t0 = 0.0, t1 = 0.0;
+      int m = 0;
+      for (; m + 1 <= r; m += 2) {
+        t0 += A[vr + m] * tb[m * i0 + c];
+        t1 += A[vr + m + 1] * tb[(m + 1) * i0 + c];
+      }
+      if (m <= r) t0 += A[vr + m] * tb[m * i0 + c];
+      A[ro32(i0 + r) + c] = -(t0 + t1);
     }
     __syncthreads();
   }
@@ -689,9 +744,17 @@ __global__ void __cluster_dims__(1, 2, 1) __launch_bounds__(kThreads) factor_ker
     if (tiles) {
       factored = chol_inv_tiles(outer, mean, N, args.loading, chain == 0, W, B, cbuf);
     } else if (inplace) {
-      fill_matrix(A, outer, mean, N, args.loading, B, chain == 0);
-      factored = cholesky_inplace(A, B, vs, &s_bad);
-      if (factored) inverse_blocked(A, A, B, lp);
+      // pointers taken straight from the shared array, so the inlined loops
+      // address shared memory directly
+      double* As = smem + B + kNb * kNb;
+      fill_matrix(As, outer, mean, N, args.loading, B, chain == 0);
+      factored = cholesky_inplace(As, B, smem + B, &s_bad);
+      if (factored) {
+        if (inplace_tb_in_smem(B))
+          inverse_inplace(As, B, As + tri(B));
+        else
+          inverse_inplace(As, B, lp);
+      }
     } else {
       fill_matrix(A, outer, mean, N, args.loading, B, chain == 0);
       factored = cholesky_blocked(A, W, B, lp, vs, &s_bad);
