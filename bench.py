@@ -1185,7 +1185,9 @@ def measure_screen(args, dist, world, rank, device):
 
     # the screen needs only the moments (its normaliser): the FP64 factorisation,
     # which the re-scoring needs, runs on a side stream under the inference
-    side = torch.cuda.Stream(device=device)
+    side = torch.cuda.Stream(device=device, priority=-1)  # the factorisation's cluster dispatches first
+    # the screen kernel one CTA short per SM of that cluster, so the two run side by side
+    screen_ctas = torch.cuda.get_device_properties(device).multi_processor_count - 2
     s_side = C.c_void_p(side.cuda_stream)
     moments_done, factor_done = torch.cuda.Event(), torch.cuda.Event()
 
@@ -1210,8 +1212,8 @@ def measure_screen(args, dist, world, rank, device):
         if ev:
             ev[1].record(stream)
         hsi.check(L.hsi_screen_normaliser(vp(moments), Bs, vp(norm), s), "normaliser")
-        hsi.check(L.hsi_screen_infer(vp(src), H, Wd, Bs, 1, stride, vp(norm), vp(screen.params), vp(logits),
-                                     vp(iws), iws.numel(), s), "screen")
+        hsi.check(L.hsi_screen_infer_ctas(vp(src), H, Wd, Bs, 1, stride, vp(norm), vp(screen.params), vp(logits),
+                                          vp(iws), iws.numel(), screen_ctas, s), "screen")
         ccount.zero_()
         hsi.check(L.hsi_detect(vp(logits), None, H, Wd, C.c_float(thr), 0, hsi.HIGHER_IS_BETTER, SCR_CAP, vp(cand),
                                vp(ccount), vp(dws), dws.numel(), s), "proposals")

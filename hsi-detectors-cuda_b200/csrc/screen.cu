@@ -759,10 +759,15 @@ extern "C" HSI_API size_t hsi_screen_infer_workspace_bytes(int bands) {
   return (sizeof(ScreenOps) + 255) & ~static_cast<size_t>(255);
 }
 
-extern "C" HSI_API int hsi_screen_infer(const void* d_cube, int height, int width, int bands, int dtype,
-                                        int64_t plane_stride, const float* d_norm, const float* d_params,
-                                        float* d_logits, void* d_workspace, size_t workspace_bytes,
-                                        hsi_stream_t stream) {
+namespace hsi_b200 {
+namespace {
+
+// Screen inference on at most max_ctas CTAs (0: one per SM).  The kernel's
+// static tile schedule covers every tile for any grid size.
+int screen_infer(const void* d_cube, int height, int width, int bands, int dtype, int64_t plane_stride,
+                 const float* d_norm, const float* d_params, float* d_logits, void* d_workspace,
+                 size_t workspace_bytes, int max_ctas, hsi_stream_t stream) {
+  if (max_ctas < 0) return HSI_E_INVALID;
   if (!d_cube || !d_norm || !d_params || !d_logits || height <= 0 || width <= 0 || bands <= 0 ||
       bands > HSI_MAX_BANDS)
     return HSI_E_INVALID;
@@ -782,11 +787,31 @@ extern "C" HSI_API int hsi_screen_infer(const void* d_cube, int height, int widt
   const cudaError_t e = raise_smem_limit(screen_tc_kernel, static_cast<int>(smem));
   if (e != cudaSuccess) return static_cast<int>(e);
   const int sms = device_sm_count();
+  const int cap = max_ctas > 0 && max_ctas < sms ? max_ctas : sms;
   const int64_t ntiles = (P + kScrTile - 1) / kScrTile;
-  const int grid = static_cast<int>(ntiles < sms ? ntiles : sms);
+  const int grid = static_cast<int>(ntiles < cap ? ntiles : cap);
   ScreenArgs a{P, Bp, ops, d_logits, nullptr};
   screen_tc_kernel<<<grid, kScrThreads, smem, s>>>(map, a);
   return static_cast<int>(cudaGetLastError());
+}
+
+}  // namespace
+}  // namespace hsi_b200
+
+extern "C" HSI_API int hsi_screen_infer(const void* d_cube, int height, int width, int bands, int dtype,
+                                        int64_t plane_stride, const float* d_norm, const float* d_params,
+                                        float* d_logits, void* d_workspace, size_t workspace_bytes,
+                                        hsi_stream_t stream) {
+  return screen_infer(d_cube, height, width, bands, dtype, plane_stride, d_norm, d_params, d_logits, d_workspace,
+                      workspace_bytes, 0, stream);
+}
+
+extern "C" HSI_API int hsi_screen_infer_ctas(const void* d_cube, int height, int width, int bands, int dtype,
+                                             int64_t plane_stride, const float* d_norm, const float* d_params,
+                                             float* d_logits, void* d_workspace, size_t workspace_bytes,
+                                             int max_ctas, hsi_stream_t stream) {
+  return screen_infer(d_cube, height, width, bands, dtype, plane_stride, d_norm, d_params, d_logits, d_workspace,
+                      workspace_bytes, max_ctas, stream);
 }
 
 extern "C" HSI_API int hsi_gather_candidates(const void* d_cube, int dtype, int64_t plane_stride, int bands,

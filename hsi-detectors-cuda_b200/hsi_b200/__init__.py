@@ -155,6 +155,7 @@ def _optional_symbols(L):
         "hsi_screen_adam": ([vp, vp, vp, i32, C.c_float, i32, vp], i32),
         "hsi_screen_infer_workspace_bytes": ([i32], C.c_size_t),
         "hsi_screen_infer": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, vp, C.c_size_t, vp], i32),
+        "hsi_screen_infer_ctas": ([vp, i32, i32, i32, i32, i64, vp, vp, vp, vp, C.c_size_t, i32, vp], i32),
         "hsi_gather_candidates": ([vp, i32, i64, i32, i32, vp, vp, i32, vp, i64, vp], i32),
         "hsi_sam_bip": ([vp, i32, i32, i32, vp, vp, i32, vp, i64, vp, vp, vp], i32),
     }

@@ -378,6 +378,14 @@ HSI_API size_t hsi_screen_infer_workspace_bytes(int bands);
 HSI_API int hsi_screen_infer(const void* d_cube, int height, int width, int bands, int dtype, int64_t plane_stride,
                              const float* d_norm, const float* d_params, float* d_logits, void* d_workspace,
                              size_t workspace_bytes, hsi_stream_t stream);
+/* hsi_screen_infer on at most max_ctas CTAs (0: one per SM), the same logits.
+ * The screen kernel is persistent, one CTA per SM; a caller that runs other
+ * work beside it (the FP64 statistics, whose cluster of two CTAs the screen
+ * does not need) caps it a few SMs short so both run at once.  No reference
+ * counterpart (the screen is this library's). */
+HSI_API int hsi_screen_infer_ctas(const void* d_cube, int height, int width, int bands, int dtype,
+                                  int64_t plane_stride, const float* d_norm, const float* d_params, float* d_logits,
+                                  void* d_workspace, size_t workspace_bytes, int max_ctas, hsi_stream_t stream);
 /* Copy the spectra of candidate pixels (a detection list and its count) into
  * a compact BSQ cube of `capacity` pixels at `out_stride`, for re-scoring;
  * slots past the count hold pixel 0. */

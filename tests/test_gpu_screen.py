@@ -107,6 +107,16 @@ def test_inference_matches_oracle(hsi, orc, B, H, W):
     ws = torch.empty(wb, dtype=torch.uint8, device="cuda")
     st = L.hsi_screen_infer(_p(cube), H, W, B, 1, stride, _p(d_norm), _p(p), _p(logits), _p(ws), wb, None)
     assert st == 0, hsi.status_string(st)
+    # the same kernel on fewer CTAs (room left for other work beside it): the same logits
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    for cap in (7, sms - 2):
+        capped = torch.full((P,), np.nan, device="cuda")
+        st = L.hsi_screen_infer_ctas(_p(cube), H, W, B, 1, stride, _p(d_norm), _p(p), _p(capped), _p(ws), wb, cap,
+                                     None)
+        assert st == 0, hsi.status_string(st)
+        assert torch.equal(capped, logits), cap
+    assert L.hsi_screen_infer_ctas(_p(cube), H, W, B, 1, stride, _p(d_norm), _p(p), _p(logits), _p(ws), wb, -1,
+                                   None) == hsi.E_INVALID
     torch.cuda.synchronize()
     feats = ((host.astype(np.float64) - mean[:, None].astype(np.float64)) * scale[:, None]).T.astype(np.float32)
     want = orc.mlp(p.cpu().numpy(), B, feats, round_bf16=True)[0]
