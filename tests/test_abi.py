@@ -108,3 +108,21 @@ def test_batch_scoring_validates_every_descriptor_before_any_launch(bad):
     assert L.hsi_score_frames_batch(C.cast(arr, C.c_void_p), len(frames), None, None) == hsi.E_INVALID
     assert L.hsi_score_frames_batch(None, 1, None, None) == hsi.E_INVALID
     assert L.hsi_score_frames_batch(C.cast(arr, C.c_void_p), 0, None, None) == hsi.E_INVALID
+
+
+def test_screen_inference_validates_arguments_before_any_launch():
+    """hsi_screen_infer / hsi_screen_infer_ctas reject bad arguments on the host,
+    before any device call, so these run without a GPU."""
+    import hsi_b200 as hsi
+    L = hsi.lib()
+    fake = C.c_void_p(1 << 40)  # 256-byte aligned, never dereferenced
+    wb = L.hsi_screen_infer_workspace_bytes(113)
+    assert wb > 0 and L.hsi_screen_infer_workspace_bytes(0) == 0
+    args = lambda cube, dtype, stride, ws: (cube, 64, 96, 113, dtype, stride, fake, fake, fake, ws, wb)  # noqa: E731
+    # a negative CTA cap, a missing cube, FP32 cubes, a plane stride short of the frame
+    assert L.hsi_screen_infer_ctas(*args(fake, hsi.F16, 6144, fake), -1, None) == hsi.E_INVALID
+    assert L.hsi_screen_infer_ctas(*args(None, hsi.F16, 6144, fake), 0, None) == hsi.E_INVALID
+    assert L.hsi_screen_infer(*args(fake, hsi.F32, 6144, fake), None) == hsi.E_INVALID
+    assert L.hsi_screen_infer_ctas(*args(fake, hsi.F16, 6000, fake), 8, None) == hsi.E_INVALID
+    # no workspace
+    assert L.hsi_screen_infer_ctas(*args(fake, hsi.F16, 6144, None), 8, None) == hsi.E_WORKSPACE
