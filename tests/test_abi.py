@@ -126,3 +126,31 @@ def test_screen_inference_validates_arguments_before_any_launch():
     assert L.hsi_screen_infer_ctas(*args(fake, hsi.F16, 6000, fake), 8, None) == hsi.E_INVALID
     # no workspace
     assert L.hsi_screen_infer_ctas(*args(fake, hsi.F16, 6144, None), 8, None) == hsi.E_WORKSPACE
+
+
+def test_statistics_sizes_and_host_side_rejections():
+    """The FP64 statistics' host-side contract: the packed layout's size, the
+    workspace (none up to 128 bands; both chains' matrices per frame above, which
+    also covers the in-place path's target vectors), and the arguments rejected
+    before any device call."""
+    import hsi_b200 as hsi
+    L = hsi.lib()
+    tri = lambda n: n * (n + 1) // 2  # noqa: E731
+    assert L.hsi_statistics_elements(113, 8) == 113 + 113 * 113 + 2 * 8 * 113 + 8
+    for B in (1, 113, 124, 128):
+        assert L.hsi_factor_workspace_bytes(3, B) == 0
+    for B in (129, 224, 238, 239, 256):
+        assert L.hsi_factor_workspace_bytes(3, B) == 8 * 4 * tri(B) * 3
+        # per frame and chain the in-place path needs the target vectors (2 x 16 x B) and at
+        # most the inverse's block-row buffer (16 x B) beside them, within 2 tri(B) doubles
+        assert 2 * 16 * B + 16 * B <= 2 * tri(B)
+    fake = C.c_void_p(1 << 40)
+    call = lambda F, B, T, loading, ws, wsb: L.hsi_build_statistics(  # noqa: E731
+        F, B, T, loading, fake, fake, 0, fake, None, None, fake, ws, wsb, None)
+    assert call(1, 224, 16, 1e-6, None, 0) == hsi.E_WORKSPACE
+    assert call(1, 224, 16, 1e-6, fake, L.hsi_factor_workspace_bytes(1, 224) - 1) == hsi.E_WORKSPACE
+    assert call(0, 113, 8, 1e-6, None, 0) == hsi.E_INVALID
+    assert call(1, 0, 8, 1e-6, None, 0) == hsi.E_INVALID
+    assert call(1, 257, 8, 1e-6, None, 0) == hsi.E_INVALID
+    assert call(1, 113, 65, 1e-6, None, 0) == hsi.E_INVALID
+    assert call(1, 113, 8, -1.0, None, 0) == hsi.E_INVALID
