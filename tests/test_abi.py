@@ -154,3 +154,32 @@ def test_statistics_sizes_and_host_side_rejections():
     assert call(1, 257, 8, 1e-6, None, 0) == hsi.E_INVALID
     assert call(1, 113, 65, 1e-6, None, 0) == hsi.E_INVALID
     assert call(1, 113, 8, -1.0, None, 0) == hsi.E_INVALID
+
+
+def test_rx_ace_and_simt_reject_bad_frames_on_the_host():
+    """RX/ACE entry points: band counts, targets, element types, strides and
+    workspaces are checked before any device call.  The tensor-core path holds
+    127 bands (more is HSI_E_CAPACITY: such frames take the plain path) and
+    scores up to 64 targets in passes; the plain path takes 16 targets a call."""
+    import hsi_b200 as hsi
+    L = hsi.lib()
+    fake = C.c_void_p(1 << 40)
+    for name in ("simt", "tc"):
+        fn = L.hsi_rx_ace_simt if name == "simt" else L.hsi_rx_ace
+        wb = (L.hsi_rx_ace_simt_workspace_bytes if name == "simt" else L.hsi_rx_ace_workspace_bytes)(113, 8)
+        assert wb > 0
+
+        def call(cube=fake, B=113, dtype=hsi.F32, stride=6144, T=8, ws=fake, wsb=wb):
+            return fn(cube, 64, 96, B, dtype, stride, fake, T, fake, fake, None, None, 6144, ws, wsb, None)
+
+        assert call(cube=None) == hsi.E_INVALID
+        assert call(B=0) == hsi.E_INVALID
+        assert call(dtype=7) == hsi.E_INVALID
+        assert call(stride=6000) == hsi.E_INVALID and call(stride=6148) == hsi.E_INVALID
+        assert call(ws=None) == hsi.E_WORKSPACE and call(wsb=wb - 1) == hsi.E_WORKSPACE
+        if name == "simt":
+            assert call(B=257) == hsi.E_INVALID
+            assert call(T=-1) == hsi.E_INVALID and call(T=17) == hsi.E_INVALID
+        else:
+            assert call(B=128) == hsi.E_CAPACITY and call(B=224) == hsi.E_CAPACITY
+            assert call(T=-1) == hsi.E_CAPACITY and call(T=65) == hsi.E_CAPACITY
