@@ -183,3 +183,23 @@ def test_rx_ace_and_simt_reject_bad_frames_on_the_host():
         else:
             assert call(B=128) == hsi.E_CAPACITY and call(B=224) == hsi.E_CAPACITY
             assert call(T=-1) == hsi.E_CAPACITY and call(T=65) == hsi.E_CAPACITY
+
+
+def test_detect_rejects_bad_jobs_on_the_host():
+    """Detection: maps, counts, capacities, polarities and workspaces are checked
+    before any device call."""
+    import hsi_b200 as hsi
+    L = hsi.lib()
+    fake = C.c_void_p(1 << 40)
+    wb = hsi.detect_workspace_bytes(64, 96)
+    assert wb > 0
+
+    def call(score=fake, count=fake, h=64, w=96, cap=16, out=fake, pol=hsi.LOWER_IS_BETTER, ws=fake, wsb=wb):
+        return L.hsi_detect(score, None, h, w, C.c_float(0.1), 2, pol, cap, out, count, ws, wsb, None)
+
+    assert call(score=None) == hsi.E_INVALID and call(count=None) == hsi.E_INVALID
+    assert call(h=0) == hsi.E_INVALID and call(w=-1) == hsi.E_INVALID
+    assert call(cap=-1) == hsi.E_INVALID and call(out=None) == hsi.E_INVALID
+    assert call(pol=2) == hsi.E_INVALID
+    assert call(ws=None) == hsi.E_WORKSPACE and call(wsb=wb - 1) == hsi.E_WORKSPACE
+    assert call(ws=C.c_void_p((1 << 40) + 4)) == hsi.E_INVALID  # workspace not on 16 bytes
