@@ -203,3 +203,32 @@ def test_detect_rejects_bad_jobs_on_the_host():
     assert call(pol=2) == hsi.E_INVALID
     assert call(ws=None) == hsi.E_WORKSPACE and call(wsb=wb - 1) == hsi.E_WORKSPACE
     assert call(ws=C.c_void_p((1 << 40) + 4)) == hsi.E_INVALID  # workspace not on 16 bytes
+
+
+def test_moments_and_bip_reject_bad_frames_on_the_host():
+    """Scene moments and the BIP scorer: frames, element types, strides,
+    alignment, outputs and workspaces are checked before any device call."""
+    import hsi_b200 as hsi
+    L = hsi.lib()
+    fake = C.c_void_p(1 << 40)
+
+    def moments(fn=L.hsi_scene_moments, cube=fake, h=64, w=96, B=113, dtype=hsi.F32, stride=6144, out=fake,
+                ws=fake, wsb=1 << 40):
+        return fn(cube, h, w, B, dtype, stride, out, None, ws, wsb, None)
+
+    assert moments(cube=None) == hsi.E_INVALID and moments(out=None) == hsi.E_INVALID
+    assert moments(B=0) == hsi.E_INVALID and moments(B=257) == hsi.E_INVALID
+    assert moments(dtype=3) == hsi.E_INVALID
+    assert moments(stride=6000) == hsi.E_INVALID and moments(stride=6148) == hsi.E_INVALID
+    assert moments(cube=C.c_void_p((1 << 40) + 8)) == hsi.E_INVALID  # cube not on 16 bytes
+    assert moments(ws=None) == hsi.E_WORKSPACE and moments(wsb=16) == hsi.E_WORKSPACE
+    assert moments(fn=L.hsi_scene_moments_tc, B=255) == hsi.E_CAPACITY  # past the limb GEMM's band views
+
+    def bip(cube=fake, B=113, T=8, maps=fake, mstride=6144, best=fake):
+        return L.hsi_sam_bip(cube, 64, 96, B, fake, fake, T, maps, mstride, best, None, None)
+
+    assert bip(cube=None) == hsi.E_INVALID and bip(B=257) == hsi.E_INVALID
+    assert bip(T=0) == hsi.E_INVALID and bip(T=65) == hsi.E_INVALID
+    assert bip(maps=None, best=None) == hsi.E_INVALID  # nothing to write
+    assert bip(mstride=6000) == hsi.E_INVALID
+    assert bip(cube=C.c_void_p((1 << 40) + 2)) == hsi.E_INVALID  # not on 4 bytes
