@@ -232,3 +232,27 @@ def test_moments_and_bip_reject_bad_frames_on_the_host():
     assert bip(maps=None, best=None) == hsi.E_INVALID  # nothing to write
     assert bip(mstride=6000) == hsi.E_INVALID
     assert bip(cube=C.c_void_p((1 << 40) + 2)) == hsi.E_INVALID  # not on 4 bytes
+
+
+def test_conversions_and_gather_reject_bad_arguments_on_the_host():
+    """Narrowing, the BIP transpose, demosaic and the candidates' gather check
+    their arguments before any device call; narrowing nothing succeeds."""
+    import hsi_b200 as hsi
+    L = hsi.lib()
+    fake = C.c_void_p(1 << 40)
+    assert L.hsi_narrow_to_half(None, None, 0, None) == hsi.OK
+    assert L.hsi_narrow_to_half(fake, fake, -1, None) == hsi.E_INVALID
+    assert L.hsi_narrow_to_half(None, fake, 8, None) == hsi.E_INVALID
+    assert L.hsi_narrow_to_half(C.c_void_p((1 << 40) + 4), fake, 8, None) == hsi.E_INVALID  # source not on 16 bytes
+    assert L.hsi_transpose_bip_to_bsq(fake, None, 8, 8, 4, 64, None) == hsi.E_INVALID
+    assert L.hsi_transpose_bip_to_bsq(fake, fake, 8, 8, 0, 64, None) == hsi.E_INVALID
+    assert L.hsi_transpose_bip_to_bsq(fake, fake, 8, 8, 4, 63, None) == hsi.E_INVALID  # stride short of the frame
+    # demosaic: more bands than mosaic cells, an unknown element type, a frame smaller than one period
+    assert L.hsi_demosaic(fake, 64, 64, 4, 17, None, fake, hsi.F32, 256, None) == hsi.E_INVALID
+    assert L.hsi_demosaic(fake, 64, 64, 4, 16, None, fake, 5, 256, None) == hsi.E_INVALID
+    assert L.hsi_demosaic(fake, 3, 64, 4, 16, None, fake, hsi.F32, 256, None) == hsi.E_INVALID
+    assert L.hsi_demosaic(fake, 64, 64, 4, 16, None, fake, hsi.F32, 255, None) == hsi.E_INVALID
+    # gather: no candidate list, an output stride short of the capacity, an unknown element type
+    assert L.hsi_gather_candidates(fake, hsi.F16, 4096, 113, 64, None, fake, 100, fake, 100, None) == hsi.E_INVALID
+    assert L.hsi_gather_candidates(fake, hsi.F16, 4096, 113, 64, fake, fake, 100, fake, 99, None) == hsi.E_INVALID
+    assert L.hsi_gather_candidates(fake, 4, 4096, 113, 64, fake, fake, 100, fake, 100, None) == hsi.E_INVALID
